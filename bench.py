@@ -1,0 +1,431 @@
+"""Benchmark of the matrix-profile self-join on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Headline workload (one GPU): c2 -- a random walk of n = 1,048,576 samples
+(seed 1), window m = 256, exclusion zone m/4, every diagonal of the distance
+matrix (5.49e11 cells).  One step = one complete self-join.  Metric: cells/s
+of the FP32 recurrence re-anchored in FP64 every K = 1024 steps, reported
+beside the plain FP64 GPU kernel on the same input and the FP32 form's
+maximum relative distance error against it.
+
+Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events
+on the stream the library launches on; an L2 flush (256 MB write) runs between
+steps outside the events; barrier + device synchronisation around the loop;
+the maximum over ranks is reported.  With N > 1 the diagonals are split into
+2N partitions, rank r taking partitions r and 2N-1-r (the reference's
+scrimp_triv_par balance rule), and the partial profiles are merged with one
+NCCL all-gather plus an element-wise arg-min.
+
+--impl reference times the reference's own CPU code (oracle/_ref, built from
+its unchanged sources; else the C restatement) on all host cores, each step a
+bounded diagonal sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MP cells/s vs plain FP64 GPU kernel at ≤1e-4 rel. error; p50/p99 solve latency"
+FLOP_PER_CELL = 8  # 2 FMA for the dot-product update, 1 FMA + 2 MUL for the score
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def diag_partitions(lo: int, hi: int, parts: int):
+    """Near-equal split of [lo, hi) into `parts` ranges (partitioning_1d.cpp:8-31)."""
+    n = hi - lo
+    full = n - (n // parts) * parts
+    size = n // parts + 1
+    out = []
+    for p in range(parts):
+        first = p * size - max(p - full, 0)
+        last = first + (size if p < full else size - 1)
+        out.append((lo + first, lo + last))
+    return out
+
+
+def sample_range(n: int, m: int, target_cells: float):
+    """Diagonal range [excl+1, hi) holding about target_cells cells."""
+    PL, lo = n - m + 1, m // 4 + 1
+    hi, cells = lo, 0.0
+    step = max(1, (PL - lo) // 4096)
+    while hi < PL and cells < target_cells:
+        h2 = min(PL, hi + step)
+        cells += sum(PL - d for d in range(hi, h2))
+        hi = h2
+    return lo, hi, cells
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = max(smax, float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def read_ncu_traffic(kernel: str):
+    """dram bytes per launch recorded in profiles/ (from one ncu capture)."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch_full:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_reference_run(x, m, target_seconds: float, threads: int):
+    """Times the reference CPU path on `threads` host threads over a diagonal
+    sample of about target_seconds.  Returns (cells, seconds, kind, sample)."""
+    from oracle.oracle import Oracle, RefOracle, build
+    n = x.size
+    kind = "reference" if RefOracle.available("ieee") else "port"
+    per_core = 1.0e9 if kind == "reference" else 4.0e8  # cells/s/core, sizing only
+    lo, hi, cells = sample_range(n, m, per_core * threads * target_seconds)
+    if kind == "reference":
+        ref = RefOracle("fast")  # the reference's release flags
+        _, _, sec = ref.triv_par_threads(x, m, lo, hi, threads)
+    else:
+        if not os.path.exists(os.path.join(ROOT, "oracle", "libscrimp_oracle.so")):
+            build(with_reference=False)
+        t0 = time.perf_counter()
+        Oracle().selfjoin(x, m, diag_lo=lo, diag_hi=hi, nthreads=threads)
+        sec = time.perf_counter() - t0
+    sample = (f"diagonals [{lo}, {hi}) of the same series: {cells:.3e} cells, "
+              f"{threads} threads, scrimp_triv_par partitioning re-hosted on threads")
+    return cells, sec, kind, sample
+
+
+def run_reference_arm(args, world):
+    import thesiscode_b200.workloads as wl
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    x, m = wl.c2()
+    threads = host_cores()
+    vals = []
+    for it in range(args.warmup + args.steps):
+        cells, sec, kind, sample = cpu_reference_run(x, m, args.ref_seconds, threads)
+        if it >= args.warmup:
+            vals.append((cells, sec))
+    cells = sum(c for c, _ in vals)
+    sec = sum(s for _, s in vals)
+    v = cells / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "cells/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sec / len(vals), "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "c2: random walk n=1,048,576 seed 1, m=256, excl=64; each step a "
+                               "bounded diagonal sample", "n": int(x.size), "m": m},
+        "cpu_baseline": {"value": v, "unit": "cells/s", "cores": threads, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": v, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world):
+    import torch
+    import torch.distributed as dist
+
+    import thesiscode_b200 as mp
+    import thesiscode_b200.workloads as wl
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if args.workload == "c1":
+        x, m = wl.c1()
+    else:
+        x, m = wl.c2()
+    n = x.size
+    PL, excl = n - m + 1, m // 4
+    lo_all, hi_all = excl + 1, PL
+    parts = diag_partitions(lo_all, hi_all, 2 * world)
+    mine = [parts[rank], parts[2 * world - 1 - rank]] if world > 1 else [(lo_all, hi_all)]
+    mine = [(a, b) for a, b in mine if b > a]
+    cells_mine = sum(mp.cells(n, m, a, b) for a, b in mine)
+    cells_total = mp.cells(n, m)
+
+    ctx = mp.Context(local)
+    ctx.set_phase_timing(True)
+    stream = torch.cuda.Stream(device=dev)
+    xd = torch.from_numpy(x).to(dev)
+    d2 = torch.empty(PL, dtype=torch.float64, device=dev)
+    ix = torch.empty(PL, dtype=torch.int64, device=dev)
+    d2b = torch.empty_like(d2)
+    ixb = torch.empty_like(ix)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def one_step(precision):
+        launches = 0
+        join_ms = 0.0
+        first = True
+        for a, b in mine:
+            tgt = (d2, ix) if first else (d2b, ixb)
+            ctx.selfjoin(xd, m, precision=precision, reanchor_k=args.reanchor_k, diag_lo=a,
+                         diag_hi=b, out=tgt, stream=stream.cuda_stream)
+            launches += ctx.last_launch_count
+            join_ms += ctx.last_phase_ms()[1]
+            if not first:
+                with torch.cuda.stream(stream):
+                    better = (d2b < d2) | ((d2b == d2) & (ixb < ix))
+                    d2.copy_(torch.where(better, d2b, d2))
+                    ix.copy_(torch.where(better, ixb, ix))
+            first = False
+        if world > 1:
+            with torch.cuda.stream(stream):
+                gd = [torch.empty_like(d2) for _ in range(world)]
+                gi = [torch.empty_like(ix) for _ in range(world)]
+                dist.all_gather(gd, d2)
+                dist.all_gather(gi, ix)
+                D = torch.stack(gd)
+                I = torch.stack(gi)
+                key_best = D.min(dim=0).values
+                cand = torch.where(D == key_best, I, torch.iinfo(torch.int64).max)
+                d2.copy_(key_best)
+                ix.copy_(cand.min(dim=0).values)
+        return launches, join_ms
+
+    def timed(precision, steps, warmup):
+        for _ in range(warmup):
+            one_step(precision)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        evs = []
+        launches = 0
+        join_ms = []
+        with ClockSampler(local) as clk:
+            for _ in range(steps):
+                with torch.cuda.stream(stream):
+                    flush.fill_(1.0)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                l, j = one_step(precision)
+                e1.record(stream)
+                evs.append((e0, e1))
+                launches += l
+                join_ms.append(j)
+            torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        per = [a.elapsed_time(b) for a, b in evs]
+        return per, launches, join_ms, clk.summary()
+
+    # -- FP32 re-anchored form (headline) ------------------------------------
+    per, launches, join_ms, clocks = timed(mp.FP32_REANCHOR, args.steps, args.warmup)
+    total_ms = sum(per)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = cells_total * args.steps / (total_ms * 1e-3)
+    fp32_d2 = d2.cpu().numpy().copy()
+    fp32_idx = ix.cpu().numpy().copy()
+
+    # -- plain FP64 GPU kernel on the same input ---------------------------------
+    fsteps = max(1, min(args.steps, args.fp64_steps))
+    per64, _, join64, _ = timed(mp.FP64, fsteps, 1)
+    tot64 = sum(per64)
+    if world > 1:
+        t = torch.tensor([tot64], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot64 = float(t.item())
+    value64 = cells_total * fsteps / (tot64 * 1e-3)
+    fp64_d2 = d2.cpu().numpy().copy()
+
+    # -- end to end through the C ABI with pinned host buffers -------------------
+    e2e = None
+    lat = None
+    if world == 1:
+        xh = torch.from_numpy(x).pin_memory()
+        oh = (torch.empty(PL, dtype=torch.float64).pin_memory(),
+              torch.empty(PL, dtype=torch.int64).pin_memory())
+        for _ in range(max(1, args.warmup)):
+            ctx.selfjoin(xh, m, precision=mp.FP32_REANCHOR, reanchor_k=args.reanchor_k, out=oh,
+                         stream=stream.cuda_stream)
+        lat = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(2.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.selfjoin(xh, m, precision=mp.FP32_REANCHOR, reanchor_k=args.reanchor_k, out=oh,
+                         stream=stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            lat.append(e0.elapsed_time(e1))
+        e2e = {"value": cells_total * len(lat) / (sum(lat) * 1e-3), "unit": "cells/s",
+               "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 16 * PL,
+               "path": "mp_selfjoin (C ABI) with pinned host input/outputs"}
+
+    if rank != 0:
+        ctx.close()
+        return
+
+    # error of the FP32 form against the FP64 kernel (bit-identical to the reference)
+    dt = np.sqrt(np.abs(fp64_d2))
+    rel = np.abs(np.sqrt(np.abs(fp32_d2)) - dt) / dt
+    err = {"max_rel": float(rel.max()), "mean_rel": float(rel.mean()),
+           "index_agreement": float(np.mean(fp32_idx == ix.cpu().numpy()))}
+
+    # roofline of the dominant kernel (the FP32 tile join)
+    join_avg_ms = float(np.mean(join_ms)) if join_ms else float("nan")
+    achieved = FLOP_PER_CELL * cells_mine / (join_avg_ms * 1e-3) / 1e12
+    peaks = {}
+    for which, name in ((0, "f32_ffma"), (1, "f32x2_ffma2"), (2, "f64_dfma")):
+        try:
+            peaks[name] = mp.measure_fma_peak(local, which) / 1e12
+        except Exception:
+            peaks[name] = None
+    peak32 = max(v for v in (peaks["f32_ffma"], peaks["f32x2_ffma2"]) if v)
+    traffic = read_ncu_traffic("fp32_tile_kernel_c2")
+    roofline = {
+        "bound": "fp32-fma-pipe (CUDA cores; no tensor-core or HBM bound)",
+        "achieved": achieved, "peak": peak32, "unit": "TFLOP/s", "frac": achieved / peak32,
+        "traffic": traffic, "kernel": "fp32_tile_kernel<8>",
+        "algorithmic_flops_per_launch": FLOP_PER_CELL * cells_mine,
+        "kernel_ms": join_avg_ms,
+        "peak_source": "measured in this run: independent-FMA-chain kernel (mp_measure_fma_peak), "
+                       "max of FFMA and f32x2 FFMA2 rates; MEASURED_PEAKS.json has no CUDA-core "
+                       "peak",
+        "peaks_tflops": peaks,
+    }
+    join64 = float(np.mean(join64)) if join64 else float("nan")
+    roof64 = FLOP_PER_CELL * cells_mine / (join64 * 1e-3) / 1e12
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{args.workload}: random walk n={n:,}, m={m}, excl={excl}, all "
+                               f"diagonals; FP32 recurrence re-anchored in FP64 every "
+                               f"K={args.reanchor_k} steps",
+                   "n": n, "m": m, "reanchor_k": args.reanchor_k, "cells": cells_total,
+                   "l2": "flushed between steps (256 MB write); working set ~100 MB",
+                   "parallelism": f"diagonal partitions x{2 * world}, NCCL all-gather merge"
+                   if world > 1 else "single GPU"},
+        "fp64_baseline": {"value": value64, "unit": "cells/s", "ms_per_step": tot64 / fsteps,
+                          "kernel": "fp64_band_kernel (reference arithmetic, bit-identical)",
+                          "roofline_frac_f64": roof64 / peaks["f64_dfma"] if peaks["f64_dfma"]
+                          else None, "kernel_ms": join64},
+        "speedup_vs_fp64": value / value64,
+        "error_vs_fp64": err,
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))}
+        if lat else None,
+        "roofline": roofline,
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if world == 1 and not args.no_cpu_baseline:
+        threads = host_cores()
+        cells, sec, kind, sample = cpu_reference_run(x, m, args.ref_seconds, threads)
+        line["cpu_baseline"] = {"value": cells / sec, "unit": "cells/s", "cores": threads,
+                                "kind": kind, "sample": sample}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["c2", "c1"], default="c2")
+    ap.add_argument("--reanchor-k", type=int, default=1024)
+    ap.add_argument("--fp64-steps", type=int, default=3)
+    ap.add_argument("--ref-seconds", type=float, default=8.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        run_reference_arm(args, world)
+        return
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, world)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

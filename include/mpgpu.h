@@ -1,0 +1,150 @@
+/*
+ * mpgpu -- B200 (sm_100a) matrix-profile self-join, C ABI.
+ *
+ * Plain C types only: pointers, sizes and status codes.  Every function
+ * returns MP_OK (0) or a positive mp_status; no C++ exception crosses this
+ * boundary.  Buffers stay owned by the caller; the library owns its device
+ * scratch through an mp_context.  One context per host thread.
+ *
+ * Semantics follow the reference's diagonal-blocked SCRIMP path
+ * (4rchangel/ThesisCode, scrimppp/):
+ *   - windows i in [0, PL), PL = n - m + 1; exclusion zone |i-j| <= excl,
+ *     excl defaults to m/4 (ScrimpVertBlocked.cpp:97);
+ *   - profile value = squared z-normalised distance 2m - 2*score
+ *     (ScrimpVertBlocked.cpp:171-174), index = nearest neighbour window;
+ *   - a window no pair improves keeps score -1 (d2 = 2m+2) and index 0
+ *     (ScrimpVertBlocked.cpp:103-104); a window of exactly zero variance
+ *     makes every score it touches NaN, so it never wins and is never chosen.
+ */
+#ifndef MPGPU_H
+#define MPGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MP_OK = 0,
+    MP_ERR_INVALID_ARG = 1,   /* n < m, m < 2, bad range, null pointer ... */
+    MP_ERR_OUT_OF_MEMORY = 2, /* device allocation failed */
+    MP_ERR_BUDGET = 3,        /* request exceeds the context's memory budget */
+    MP_ERR_CUDA = 4,          /* a CUDA call failed; see mp_last_error() */
+    MP_ERR_NOT_SUPPORTED = 5, /* size or option outside what is implemented */
+    MP_ERR_NO_DEVICE = 6      /* no usable sm_100 device */
+} mp_status;
+
+typedef enum {
+    /* Operation-for-operation replica of the reference arithmetic in FP64:
+     * same window statistics, same first dot products, same fused /
+     * separately rounded per-cell steps as the reference's AVX2 kernel.
+     * Profile values are bit-identical to the reference compiled with IEEE
+     * semantics; indices agree except between candidates whose squared
+     * distances tie to within 2^-29 relative (n <= 2^23). */
+    MP_PREC_FP64 = 0,
+    /* FP32 covariance recurrence re-anchored every reanchor_k steps by an FP64
+     * dot product; window means/norms in FP64 (Welford). */
+    MP_PREC_FP32_REANCHOR = 1
+} mp_precision;
+
+typedef struct mp_context mp_context;
+
+/* device: CUDA ordinal.  mem_budget_bytes: ceiling for the context's device
+ * scratch (0 = no ceiling); a call that would exceed it fails with
+ * MP_ERR_BUDGET before allocating. */
+int mp_context_create(int device, size_t mem_budget_bytes, mp_context** out);
+int mp_context_destroy(mp_context* ctx);
+/* Text of the last error recorded on ctx (never NULL). */
+const char* mp_last_error(const mp_context* ctx);
+const char* mp_status_string(int status);
+/* Device bytes one self-join of (n, m, precision) needs in ctx's scratch. */
+size_t mp_selfjoin_scratch_bytes(int64_t n, int64_t m, int precision);
+
+/*
+ * Whole self-join (replaces ScrimpVertBlocked::compute_matrix_profile,
+ * scrimppp/src/ScrimpVertBlocked.cpp:89-195, minus the file I/O).
+ *
+ *   A            n doubles, host or device memory (detected).
+ *   excl         exclusion zone; < 0 selects m/4.
+ *   precision    mp_precision.
+ *   reanchor_k   FP32 form: columns between FP64 re-anchors (0 = 1024).
+ *   blocklen     FP64 form: the reference's --blocklen (0 = 500); it decides
+ *                which cells the reference evaluates with fused operations,
+ *                so it is needed for bit-identical values.
+ *   diag_lo/hi   evaluate diagonals [diag_lo, diag_hi) only (0,0 = all,
+ *                i.e. excl+1 .. PL-1); used for sharding and for sampling.
+ *   dist2_out    PL doubles: squared distances (host or device).
+ *   idx_out      PL int64 neighbour indices (host or device).
+ *   stream       cudaStream_t (NULL = legacy default stream).
+ * The call returns after the results are written (it synchronises stream).
+ */
+int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t excl,
+                int precision, int64_t reanchor_k, int64_t blocklen, int64_t diag_lo,
+                int64_t diag_hi, double* dist2_out, int64_t* idx_out, void* stream);
+
+/*
+ * One block of diagonals, the reference's kernel interface
+ * (scrimppp/inc/kernels.h:7-24, scrimppp/src/kernels.cpp:368-410), evaluated
+ * on the GPU in FP64 with the reference's per-cell arithmetic.  Arguments have
+ * the reference's meaning: a triangle of `blocklen` adjacent diagonals and
+ * `trianglen` columns; column j meets rows i = j + delta, delta < blocklen,
+ * i < trianglen; scores (not distances) are max-merged with strict '>' into
+ * prof_colmin[j]/idx_colmin[j] (neighbour i + baserow) and
+ * prof_rowmin[i]/idx_rowmin[i] (neighbour j + basecol); tmpQ[delta] carries
+ * the running dot product in and out.  The two profile views may alias one
+ * array (self-join) or be disjoint (tiles).  Host or device pointers; all in
+ * the same memory space.  Synchronous on stream.
+ */
+int mp_eval_diag_block_triangle(mp_context* ctx, double* prof_colmin, int64_t* idx_colmin,
+                                double* prof_rowmin, int64_t* idx_rowmin, double* tmpQ,
+                                int64_t blocklen, int64_t trianglen, const double* A_hor,
+                                const double* A_vert, int64_t m, const double* s_hor,
+                                const double* mu_hor, const double* s_vert, const double* mu_vert,
+                                int64_t baserow, int64_t basecol, void* stream);
+
+/* Window statistics of the reference (ScrimpSequOpt.cpp:33-79), bit-identical:
+ * muS[i] = mean*sInv*sqrt(m), sInv[i] = 1/sqrt(var), i < PL. */
+int mp_window_stats(mp_context* ctx, const double* A, int64_t n, int64_t m, double* muS,
+                    double* sInv, void* stream);
+
+/* First dot products of diagonals [d_lo, d_hi) (ScrimpSequOpt.cpp:81-96),
+ * bit-identical: qt[d - d_lo] = sum_k A[k+d]*A[k] summed in k order. */
+int mp_first_qt(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t d_lo,
+                int64_t d_hi, double* qt, void* stream);
+
+/* Kernel launches the last call on ctx made (for launch accounting). */
+int64_t mp_last_launch_count(const mp_context* ctx);
+
+/* Phase timing: with on != 0, mp_selfjoin records CUDA events on its stream
+ * around its three phases (preparation, join kernel, finalisation);
+ * mp_last_phase_ms reads them after the call (milliseconds, -1 if unset). */
+int mp_set_phase_timing(mp_context* ctx, int on);
+int mp_last_phase_ms(const mp_context* ctx, double* prep_ms, double* join_ms,
+                     double* finalize_ms);
+
+/* FMA throughput of this device's CUDA-core pipes in FLOP/s (2 per FMA),
+ * measured with independent FMA chains: which = 0 FP32 (FFMA), 1 FP32 (f32x2
+ * FFMA2), 2 FP64 (DFMA).  The join kernels' compute roofline uses it. */
+int mp_measure_fma_peak(int device, int which, double* flops_per_s);
+
+/*
+ * Algorithm registry (the reference's MatProfImplFactory,
+ * scrimppp/src/MatProfAlgo.cpp:11-37, exposed to C callers).
+ * mp_list_algorithms writes the space-separated registered names into buf and
+ * returns the length needed including the terminator.
+ * mp_run_algorithm runs one registered variant end to end on files, like the
+ * reference's main (scrimppp/src/main.cpp:47-80): filetype 1 = ASCII,
+ * 2 = binary; blocklen/reanchor_k <= 0 keep the defaults (500 / 1024).
+ */
+int mp_list_algorithms(char* buf, size_t len);
+int mp_run_algorithm(const char* algo, const char* input_file, const char* output_file,
+                     int window_length, int prescrimp_stride, int blocklen, int filetype,
+                     int64_t reanchor_k, int device);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPGPU_H */

@@ -1,0 +1,58 @@
+"""Shared fixtures.  `-m gpu` tests need a B200 and the in-tree libmpgpu.so;
+everything else runs on CPU."""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 GPU and the built CUDA library")
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle.oracle import Oracle, build
+    if not os.path.exists(os.path.join(ROOT, "oracle", "libscrimp_oracle.so")):
+        build(with_reference=False)
+    return Oracle()
+
+
+@pytest.fixture(scope="session")
+def golden_ascii():
+    return dict(np.load(os.path.join(GOLDEN, "test_ascii.npz")))
+
+
+@pytest.fixture(scope="session")
+def golden_edges():
+    z = np.load(os.path.join(GOLDEN, "edge_cases.npz"))
+    cases = {}
+    for k in z.files:
+        name, field = k.split("__")
+        cases.setdefault(name, {})[field] = z[k]
+    return cases
+
+
+@pytest.fixture(scope="session")
+def digests():
+    return json.load(open(os.path.join(GOLDEN, "digests.json")))
+
+
+@pytest.fixture(scope="session")
+def gpu_ctx():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("gpu test on a host without CUDA")
+    import thesiscode_b200 as mp
+    ctx = mp.Context(0)
+    yield ctx
+    ctx.close()

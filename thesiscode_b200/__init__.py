@@ -1,0 +1,256 @@
+"""thesiscode_b200 -- B200-native matrix-profile self-join.
+
+Python front end of the in-tree C-ABI library ``libmpgpu.so``
+(include/mpgpu.h).  The kernels are hand-written CUDA for sm_100a; this
+module only moves arguments across the C boundary.  There is no CPU fallback:
+every call that needs the library fails loudly when it is missing or when no
+B200 is present.
+
+The names mirror the reference's interface (4rchangel/ThesisCode, scrimppp/):
+``selfjoin`` is ScrimpVertBlocked::compute_matrix_profile without file I/O,
+``eval_diag_block_triangle`` is the reference kernel (inc/kernels.h:7-24),
+``window_stats``/``first_qt`` are ScrimpSequOpt's helpers, and
+``list_algorithms``/``run_algorithm`` drive the algorithm-variant factory
+(inc/MatProfAlgo.hpp) through the C++ host layer.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmpgpu.so")
+CLI_PATH = os.path.join(HERE, "mpgpu_cli")
+
+MP_OK = 0
+MP_ERR_INVALID_ARG = 1
+MP_ERR_OUT_OF_MEMORY = 2
+MP_ERR_BUDGET = 3
+MP_ERR_CUDA = 4
+MP_ERR_NOT_SUPPORTED = 5
+MP_ERR_NO_DEVICE = 6
+
+FP64 = 0
+FP32_REANCHOR = 1
+
+FILETYPE_ASCII = 1
+FILETYPE_BIN = 2
+
+# Every extern "C" symbol include/mpgpu.h declares.
+EXPORTED_SYMBOLS = (
+    "mp_context_create", "mp_context_destroy", "mp_last_error", "mp_status_string",
+    "mp_selfjoin_scratch_bytes", "mp_selfjoin", "mp_eval_diag_block_triangle",
+    "mp_window_stats", "mp_first_qt", "mp_last_launch_count", "mp_list_algorithms",
+    "mp_run_algorithm", "mp_set_phase_timing", "mp_last_phase_ms", "mp_measure_fma_peak",
+)
+
+
+class MpError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+_lib = None
+_P = ctypes.c_void_p
+_i64 = ctypes.c_int64
+
+
+def load_library() -> ctypes.CDLL:
+    """Loads libmpgpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(
+            f"{LIB_PATH} is missing; build it with `python -m thesiscode_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    L.mp_context_create.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(_P)]
+    L.mp_context_destroy.argtypes = [_P]
+    L.mp_last_error.argtypes = [_P]
+    L.mp_last_error.restype = ctypes.c_char_p
+    L.mp_status_string.argtypes = [ctypes.c_int]
+    L.mp_status_string.restype = ctypes.c_char_p
+    L.mp_selfjoin_scratch_bytes.argtypes = [_i64, _i64, ctypes.c_int]
+    L.mp_selfjoin_scratch_bytes.restype = ctypes.c_size_t
+    L.mp_selfjoin.argtypes = [_P, _P, _i64, _i64, _i64, ctypes.c_int, _i64, _i64, _i64, _i64,
+                              _P, _P, _P]
+    L.mp_eval_diag_block_triangle.argtypes = [_P, _P, _P, _P, _P, _P, _i64, _i64, _P, _P, _i64,
+                                              _P, _P, _P, _P, _i64, _i64, _P]
+    L.mp_window_stats.argtypes = [_P, _P, _i64, _i64, _P, _P, _P]
+    L.mp_first_qt.argtypes = [_P, _P, _i64, _i64, _i64, _i64, _P, _P]
+    L.mp_last_launch_count.argtypes = [_P]
+    L.mp_last_launch_count.restype = _i64
+    L.mp_set_phase_timing.argtypes = [_P, ctypes.c_int]
+    L.mp_last_phase_ms.argtypes = [_P, ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double)]
+    L.mp_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.mp_list_algorithms.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+    L.mp_run_algorithm.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   _i64, ctypes.c_int]
+    _lib = L
+    return L
+
+
+def status_string(status: int) -> str:
+    return load_library().mp_status_string(status).decode()
+
+
+def list_algorithms() -> list[str]:
+    L = load_library()
+    buf = ctypes.create_string_buffer(4096)
+    L.mp_list_algorithms(buf, len(buf))
+    return buf.value.decode().split()
+
+
+def run_algorithm(algo: str, input_file: str, output_file: str, window_length: int,
+                  prescrimp_stride: int = 0, blocklen: int = 0, filetype: int = FILETYPE_ASCII,
+                  reanchor_k: int = 0, device: int = 0) -> int:
+    """One registered variant end to end on files (the reference's main)."""
+    L = load_library()
+    return L.mp_run_algorithm(algo.encode(), input_file.encode(), output_file.encode(),
+                              window_length, prescrimp_stride, blocklen, filetype, reanchor_k,
+                              device)
+
+
+def measure_fma_peak(device: int = 0, which: int = 1) -> float:
+    """FLOP/s of the CUDA-core FMA pipe: 0 FP32 FFMA, 1 FP32 f32x2, 2 FP64."""
+    v = ctypes.c_double()
+    rc = load_library().mp_measure_fma_peak(device, which, ctypes.byref(v))
+    if rc != MP_OK:
+        raise MpError(rc, status_string(rc))
+    return v.value
+
+
+def _ptr(a) -> int | None:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a.data_ptr())  # torch tensor (device or host)
+
+
+@dataclass
+class Profile:
+    dist2: object   # squared distances (numpy or torch)
+    index: object   # neighbour windows
+
+    @property
+    def distance(self):
+        return np.sqrt(np.abs(np.asarray(self.dist2)))
+
+
+class Context:
+    """One mp_context: a device and its scratch (one per host thread)."""
+
+    def __init__(self, device: int = 0, mem_budget_bytes: int = 0):
+        L = load_library()
+        h = _P()
+        rc = L.mp_context_create(device, mem_budget_bytes, ctypes.byref(h))
+        if rc != MP_OK:
+            raise MpError(rc, status_string(rc))
+        self._h = h
+        self._L = L
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.mp_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != MP_OK:
+            raise MpError(rc, f"{status_string(rc)}: {self._L.mp_last_error(self._h).decode()}")
+
+    def set_phase_timing(self, on: bool = True):
+        self._check(self._L.mp_set_phase_timing(self._h, int(on)))
+
+    def last_phase_ms(self) -> tuple[float, float, float]:
+        """(preparation, join kernel, finalisation) of the last selfjoin, in ms."""
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(self._L.mp_last_phase_ms(self._h, ctypes.byref(a), ctypes.byref(b),
+                                             ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    @property
+    def last_launch_count(self) -> int:
+        return int(self._L.mp_last_launch_count(self._h))
+
+    def selfjoin(self, A, m: int, precision: int = FP64, reanchor_k: int = 0,
+                 blocklen: int = 0, diag_lo: int = 0, diag_hi: int = 0, excl: int = -1,
+                 out=None, stream=None) -> Profile:
+        """Self-join of series A (numpy float64 on the host, or a CUDA tensor).
+
+        Returns squared distances and neighbour indices for every window, in the
+        memory space of ``out`` (numpy arrays by default)."""
+        if isinstance(A, np.ndarray):
+            A = np.ascontiguousarray(A, dtype=np.float64)
+            n = A.size
+        else:
+            n = A.numel()
+        PL = n - m + 1
+        if out is None:
+            d2 = np.empty(max(PL, 0), dtype=np.float64)
+            ix = np.empty(max(PL, 0), dtype=np.int64)
+        else:
+            d2, ix = out
+        rc = self._L.mp_selfjoin(self._h, _ptr(A), n, m, excl, precision, reanchor_k, blocklen,
+                                 diag_lo, diag_hi, _ptr(d2), _ptr(ix), stream)
+        self._check(rc)
+        return Profile(d2, ix)
+
+    def window_stats(self, A, m: int):
+        A = np.ascontiguousarray(A, dtype=np.float64)
+        PL = A.size - m + 1
+        muS = np.empty(PL)
+        sInv = np.empty(PL)
+        self._check(self._L.mp_window_stats(self._h, _ptr(A), A.size, m, _ptr(muS), _ptr(sInv),
+                                            None))
+        return muS, sInv
+
+    def first_qt(self, A, m: int, d_lo: int, d_hi: int):
+        A = np.ascontiguousarray(A, dtype=np.float64)
+        qt = np.empty(max(d_hi - d_lo, 0))
+        self._check(self._L.mp_first_qt(self._h, _ptr(A), A.size, m, d_lo, d_hi, _ptr(qt),
+                                        None))
+        return qt
+
+    def eval_diag_block_triangle(self, prof_colmin, idx_colmin, prof_rowmin, idx_rowmin, tmpQ,
+                                 blocklen, trianglen, A_hor, A_vert, m, s_hor, mu_hor, s_vert,
+                                 mu_vert, baserow, basecol):
+        """The reference kernel's contract; numpy views are updated in place."""
+        self._check(self._L.mp_eval_diag_block_triangle(
+            self._h, _ptr(prof_colmin), _ptr(idx_colmin), _ptr(prof_rowmin), _ptr(idx_rowmin),
+            _ptr(tmpQ), blocklen, trianglen, _ptr(A_hor), _ptr(A_vert), m, _ptr(s_hor),
+            _ptr(mu_hor), _ptr(s_vert), _ptr(mu_vert), baserow, basecol, None))
+
+
+def cells(n: int, m: int, diag_lo: int = 0, diag_hi: int = 0, excl: int = -1) -> int:
+    """Distance-matrix cells a self-join evaluates on diagonals [diag_lo, diag_hi)."""
+    PL = n - m + 1
+    excl = m // 4 if excl < 0 else excl
+    if diag_lo == 0 and diag_hi == 0:
+        diag_lo, diag_hi = excl + 1, PL
+    diag_lo = max(diag_lo, excl + 1)
+    diag_hi = min(diag_hi, PL)
+    if diag_hi <= diag_lo:
+        return 0
+    a, b = PL - diag_lo, PL - diag_hi + 1  # lengths of first and last diagonal
+    return (a + b) * (diag_hi - diag_lo) // 2

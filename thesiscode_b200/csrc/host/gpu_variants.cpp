@@ -1,0 +1,151 @@
+// GPU algorithm variants registered in the reference's factory interface.
+//
+//   gpu_vert_blocked_fp64   drop-in for scrimp_vert_blocked
+//                           (scrimppp/src/ScrimpVertBlocked.cpp:89-195): same
+//                           input/output files and values, computed on the GPU
+//                           with the reference's FP64 arithmetic.
+//   gpu_vert_blocked_fp32k  FP32 recurrence re-anchored in FP64 every
+//                           reanchor_k steps.
+//
+// Both read the series (ASCII or binary, ScrimpSequ.hpp:91-112), run one
+// self-join through mp_selfjoin and store the profile like
+// ScrimpSequ::store_matrix_profile (ScrimpSequ.cpp:375-309).
+#include <chrono>
+#include <cstring>
+#include <iomanip>
+#include <iostream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "mpgpu.h"
+#include "matprof_algo.hpp"
+#include "profile_io.hpp"
+
+namespace matrix_profile {
+
+namespace {
+
+std::vector<double> fetch_series(const Scrimppp_params& p) {
+    switch (p.filetype) {
+        case Scrimppp_params::ASCII: return io::read_series_ascii(p.time_series_filename);
+        case Scrimppp_params::BIN: return io::read_series_bin(p.time_series_filename);
+        default: throw std::runtime_error("Unhandled file type detected.");
+    }
+}
+
+void store_profile(const Scrimppp_params& p, const std::vector<double>& d2,
+                   const std::vector<int64_t>& idx) {
+    if (p.output_filename.empty()) throw std::runtime_error("Empty output file name specified!");
+    switch (p.filetype) {
+        case Scrimppp_params::ASCII:
+            io::write_profile_ascii(p.output_filename, d2.data(), idx.data(), (int64_t)d2.size());
+            break;
+        case Scrimppp_params::BIN:
+            io::write_profile_bin(p.output_filename, d2.data(), idx.data(), (int64_t)d2.size());
+            break;
+        default: throw std::runtime_error("Unhandled file type detected.");
+    }
+}
+
+class GpuVertBlocked : public IMatProfAlgo {
+public:
+    explicit GpuVertBlocked(int precision) : precision_(precision) {}
+    ~GpuVertBlocked() override {
+        if (ctx_) mp_context_destroy(ctx_);
+    }
+    void initialize(const Scrimppp_params& params) override {
+        if (ctx_) return;
+        const int rc = mp_context_create(params.device, params.mem_budget_bytes, &ctx_);
+        if (rc != MP_OK)
+            throw std::runtime_error(std::string("mp_context_create: ") + mp_status_string(rc));
+    }
+    void compute_matrix_profile(const Scrimppp_params& params) override {
+        initialize(params);
+        const std::vector<double> A = fetch_series(params);
+        const int64_t n = (int64_t)A.size(), m = params.query_window_len;
+        if (m < 2 || n < m)
+            throw std::invalid_argument(
+                "ERROR: Time series is shorter than the window length, can not proceed");
+        const int64_t PL = n - m + 1;
+        std::vector<double> d2(PL);
+        std::vector<int64_t> idx(PL);
+        const auto t0 = std::chrono::steady_clock::now();
+        const int rc = mp_selfjoin(ctx_, A.data(), n, m, -1, precision_, params.reanchor_k,
+                                   params.block_length, 0, 0, d2.data(), idx.data(), nullptr);
+        const double sec =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (rc != MP_OK)
+            throw std::runtime_error(std::string("mp_selfjoin: ") + mp_status_string(rc) + ": " +
+                                     mp_last_error(ctx_));
+        const double excl = (double)(m / 4);
+        const double tri = (double)PL - excl;
+        std::clog << "total computation time: " << std::setprecision(17) << sec << " seconds."
+                  << std::endl;
+        std::clog << "throughput computations: " << tri * tri / sec << " matrix entries/second"
+                  << std::endl;
+        std::clog << "true cells/second: " << (tri - 1.0) * tri / 2.0 / sec << std::endl;
+        store_profile(params, d2, idx);
+    }
+
+private:
+    int precision_;
+    mp_context* ctx_ = nullptr;
+};
+
+class GpuVertBlockedFp64 : public GpuVertBlocked {
+public:
+    GpuVertBlockedFp64() : GpuVertBlocked(MP_PREC_FP64) {}
+};
+class GpuVertBlockedFp32K : public GpuVertBlocked {
+public:
+    GpuVertBlockedFp32K() : GpuVertBlocked(MP_PREC_FP32_REANCHOR) {}
+};
+
+FactoryRegistration<GpuVertBlockedFp64> reg_fp64("gpu_vert_blocked_fp64");
+FactoryRegistration<GpuVertBlockedFp32K> reg_fp32("gpu_vert_blocked_fp32k");
+
+}  // namespace
+
+}  // namespace matrix_profile
+
+using matrix_profile::MatProfImplFactory;
+using matrix_profile::Scrimppp_params;
+
+extern "C" int mp_list_algorithms(char* buf, size_t len) {
+    const std::string s = MatProfImplFactory::getInstance().get_available_implementations();
+    if (!buf || len == 0) return (int)s.size() + 1;
+    std::strncpy(buf, s.c_str(), len - 1);
+    buf[len - 1] = '\0';
+    return (int)s.size() + 1;
+}
+
+extern "C" int mp_run_algorithm(const char* algo, const char* input_file, const char* output_file,
+                                int window_length, int prescrimp_stride, int blocklen,
+                                int filetype, int64_t reanchor_k, int device) {
+    if (!algo || !input_file || !output_file) return MP_ERR_INVALID_ARG;
+    Scrimppp_params p;
+    p.algo_name = algo;
+    p.time_series_filename = input_file;
+    p.output_filename = output_file;
+    p.query_window_len = window_length;
+    p.prescrimp_stride = prescrimp_stride;
+    if (blocklen > 0) p.block_length = blocklen;
+    p.filetype = filetype == 2 ? Scrimppp_params::BIN : Scrimppp_params::ASCII;
+    if (reanchor_k > 0) p.reanchor_k = (long)reanchor_k;
+    p.device = device;
+    try {
+        auto a = MatProfImplFactory::getInstance().create(p.algo_name);
+        a->initialize(p);
+        a->compute_matrix_profile(p);
+        a->log_info();
+    } catch (const std::out_of_range&) {
+        return MP_ERR_INVALID_ARG;
+    } catch (const std::invalid_argument&) {
+        return MP_ERR_INVALID_ARG;
+    } catch (const std::exception& e) {
+        std::cerr << "mp_run_algorithm: " << e.what() << std::endl;
+        return MP_ERR_CUDA;
+    }
+    return MP_OK;
+}

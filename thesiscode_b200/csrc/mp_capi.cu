@@ -1,0 +1,662 @@
+// C ABI of the mpgpu library (declared in include/mpgpu.h).
+//
+// Host-side orchestration only: argument checks, device scratch, copies for
+// host-resident buffers, and the launch sequence of each entry point.  No
+// arithmetic of the profile happens on the host.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mpgpu.h"
+#include "mp_common.cuh"
+#include "mp_kernels.h"
+
+using namespace mpgpu;
+
+struct mp_context {
+    int device = 0;
+    size_t budget = 0;
+    std::string last_error;
+    int64_t launches = 0;
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    bool timing = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    double phase_ms[3] = {-1.0, -1.0, -1.0};
+};
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int64_t kFp64Pad = 64 * 8 + 64;  // records past the end: 32*R + 2R rows, R <= 8
+constexpr int kFp32R = 8;
+constexpr int64_t kFp32Pad = 64 * 8 + 64;
+
+int fail(mp_context* ctx, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->last_error = buf;
+    return code;
+}
+
+#define MP_CUDA(ctx, call)                                                                 \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(ctx, MP_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+#define MP_LAUNCHED(ctx)                                                                  \
+    do {                                                                                  \
+        ++(ctx)->launches;                                                                \
+        cudaError_t e_ = cudaGetLastError();                                              \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(ctx, MP_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e_)); \
+    } while (0)
+
+unsigned grid_for(int64_t count) {
+    int64_t b = (count + kThreads - 1) / kThreads;
+    if (b < 1) b = 1;
+    if (b > 148 * 32) b = 148 * 32;
+    return (unsigned)b;
+}
+
+size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Carves typed sub-buffers out of the context arena.
+struct Carve {
+    char* base;
+    size_t off = 0;
+    template <class T>
+    T* take(int64_t count) {
+        T* p = reinterpret_cast<T*>(base + off);
+        off += align_up(sizeof(T) * (size_t)std::max<int64_t>(count, 1));
+        return p;
+    }
+};
+
+int reserve(mp_context* ctx, size_t bytes) {
+    if (ctx->budget && bytes > ctx->budget)
+        return fail(ctx, MP_ERR_BUDGET, "request needs %zu bytes of device scratch, budget is %zu",
+                    bytes, ctx->budget);
+    if (bytes <= ctx->arena_bytes) return MP_OK;
+    if (ctx->arena) cudaFree(ctx->arena);
+    ctx->arena = nullptr;
+    ctx->arena_bytes = 0;
+    cudaError_t e = cudaMalloc(&ctx->arena, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, MP_ERR_OUT_OF_MEMORY, "cudaMalloc(%zu) failed: %s", bytes,
+                    cudaGetErrorString(e));
+    }
+    ctx->arena_bytes = bytes;
+    return MP_OK;
+}
+
+bool on_device(const void* p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+int bits_for(uint64_t maxval) {
+    int b = 1;
+    while (b < 63 && (1ull << b) <= maxval) ++b;
+    return b;
+}
+
+unsigned host_ord_f32(float v) {
+    unsigned b;
+    std::memcpy(&b, &v, 4);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+int fp64_shards(int64_t PL) {
+    const double per = 16.0 * (double)PL;
+    int64_t s = (int64_t)(4.0e9 / per);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(32, s));
+}
+
+// Warps in flight wanted per launch: 148 SMs x 12 resident warps.
+int pick_fp64_R(int64_t ndiag) {
+    const int64_t want = 148 * 12;
+    for (int R : {8, 4, 2}) {
+        const int64_t nb = (ndiag + 32 * R - 1) / (32 * R);
+        if ((nb + 1) / 2 >= want) return R;
+    }
+    return 1;
+}
+
+int launch_band(int R, const Fp64BandParams& P, cudaStream_t s) {
+    switch (R) {
+        case 8: launch_fp64_band<8>(P, s); break;
+        case 4: launch_fp64_band<4>(P, s); break;
+        case 2: launch_fp64_band<2>(P, s); break;
+        default: launch_fp64_band<1>(P, s); break;
+    }
+    return 0;
+}
+
+struct Sizes {
+    int64_t n, m, PL, excl, lo, hi;
+};
+
+int check_join_args(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t excl,
+                    int64_t diag_lo, int64_t diag_hi, double* d2, int64_t* idx, Sizes& S) {
+    if (!ctx) return MP_ERR_INVALID_ARG;
+    if (!A || !d2 || !idx) return fail(ctx, MP_ERR_INVALID_ARG, "null buffer");
+    if (m < 2) return fail(ctx, MP_ERR_INVALID_ARG, "window length m=%lld < 2", (long long)m);
+    if (n < m)
+        return fail(ctx, MP_ERR_INVALID_ARG,
+                    "time series is shorter than the window length (n=%lld, m=%lld)",
+                    (long long)n, (long long)m);
+    if (n - m + 1 >= (1ll << 31))
+        return fail(ctx, MP_ERR_NOT_SUPPORTED, "profile length %lld exceeds 2^31-1",
+                    (long long)(n - m + 1));
+    S.n = n;
+    S.m = m;
+    S.PL = n - m + 1;
+    S.excl = excl < 0 ? m / 4 : excl;
+    S.lo = diag_lo;
+    S.hi = diag_hi;
+    if (S.lo == 0 && S.hi == 0) {
+        S.lo = S.excl + 1;
+        S.hi = S.PL;
+    }
+    S.lo = std::max<int64_t>(S.lo, S.excl + 1);
+    S.hi = std::min<int64_t>(S.hi, S.PL);
+    if (S.hi < S.lo) S.hi = S.lo;
+    return MP_OK;
+}
+
+size_t fp64_scratch(int64_t n, int64_t m, int64_t ndiag, bool host_io) {
+    const int64_t PL = n - m + 1;
+    const int S = fp64_shards(PL);
+    size_t b = 0;
+    b += align_up(8 * (size_t)(n + 1));          // Apad
+    b += 2 * align_up(8 * (size_t)n);            // prefix sums
+    b += 2 * align_up(8 * (size_t)PL);           // muS, sInv
+    b += align_up(8 * (size_t)std::max<int64_t>(ndiag, 1));  // first QT
+    b += align_up(32 * (size_t)(PL + kFp64Pad)); // records
+    b += 2 * align_up(8 * (size_t)PL * S);       // keys
+    if (host_io) b += align_up(8 * (size_t)PL) * 2;
+    return b + 4096;
+}
+
+size_t fp32_scratch(int64_t n, int64_t m, bool host_io) {
+    const int64_t PL = n - m + 1;
+    size_t b = 0;
+    b += align_up(8 * (size_t)(n + kFp32Pad));   // Apad
+    b += align_up(4 * (size_t)n);                // change counts
+    b += align_up(4 * (size_t)((n + kThreads - 1) / kThreads + 1));
+    b += 2 * align_up(8 * (size_t)(PL + kFp32Pad));  // mean, norm
+    b += 2 * align_up(32 * (size_t)(PL + kFp32Pad)); // row/col records
+    b += align_up(8 * (size_t)PL);               // keys
+    if (host_io) b += align_up(8 * (size_t)PL) * 2;
+    return b + 4096;
+}
+
+void mark(mp_context* ctx, int k, cudaStream_t st) {
+    if (!ctx->timing) return;
+    if (!ctx->ev[k]) cudaEventCreate(&ctx->ev[k]);
+    cudaEventRecord(ctx->ev[k], st);
+}
+
+void collect_phases(mp_context* ctx) {
+    for (int k = 0; k < 3; ++k) ctx->phase_ms[k] = -1.0;
+    if (!ctx->timing) return;
+    for (int k = 0; k < 3; ++k) {
+        float ms = 0.f;
+        if (ctx->ev[k] && ctx->ev[k + 1] && cudaEventElapsedTime(&ms, ctx->ev[k], ctx->ev[k + 1]) == cudaSuccess)
+            ctx->phase_ms[k] = ms;
+        else
+            cudaGetLastError();
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int mp_set_phase_timing(mp_context* ctx, int on) {
+    if (!ctx) return MP_ERR_INVALID_ARG;
+    ctx->timing = on != 0;
+    return MP_OK;
+}
+
+int mp_last_phase_ms(const mp_context* ctx, double* prep_ms, double* join_ms, double* finalize_ms) {
+    if (!ctx) return MP_ERR_INVALID_ARG;
+    if (prep_ms) *prep_ms = ctx->phase_ms[0];
+    if (join_ms) *join_ms = ctx->phase_ms[1];
+    if (finalize_ms) *finalize_ms = ctx->phase_ms[2];
+    return MP_OK;
+}
+
+const char* mp_status_string(int status) {
+    switch (status) {
+        case MP_OK: return "ok";
+        case MP_ERR_INVALID_ARG: return "invalid argument";
+        case MP_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case MP_ERR_BUDGET: return "request exceeds the memory budget";
+        case MP_ERR_CUDA: return "CUDA error";
+        case MP_ERR_NOT_SUPPORTED: return "not supported";
+        case MP_ERR_NO_DEVICE: return "no usable device";
+        default: return "unknown status";
+    }
+}
+
+int mp_context_create(int device, size_t mem_budget_bytes, mp_context** out) {
+    if (!out) return MP_ERR_INVALID_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= device || device < 0) {
+        cudaGetLastError();
+        return MP_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) {
+        cudaGetLastError();
+        return MP_ERR_NO_DEVICE;
+    }
+    mp_context* c = new mp_context();
+    c->device = device;
+    c->budget = mem_budget_bytes;
+    *out = c;
+    return MP_OK;
+}
+
+int mp_context_destroy(mp_context* ctx) {
+    if (!ctx) return MP_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    if (ctx->arena) cudaFree(ctx->arena);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    delete ctx;
+    return MP_OK;
+}
+
+const char* mp_last_error(const mp_context* ctx) {
+    return ctx ? ctx->last_error.c_str() : "no context";
+}
+
+int64_t mp_last_launch_count(const mp_context* ctx) { return ctx ? ctx->launches : -1; }
+
+size_t mp_selfjoin_scratch_bytes(int64_t n, int64_t m, int precision) {
+    if (m < 2 || n < m) return 0;
+    if (precision == MP_PREC_FP64) return fp64_scratch(n, m, n - m + 1, true);
+    return fp32_scratch(n, m, true);
+}
+
+int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t excl,
+                int precision, int64_t reanchor_k, int64_t blocklen, int64_t diag_lo,
+                int64_t diag_hi, double* dist2_out, int64_t* idx_out, void* stream) {
+    Sizes S;
+    int rc = check_join_args(ctx, A, n, m, excl, diag_lo, diag_hi, dist2_out, idx_out, S);
+    if (rc) return rc;
+    if (precision != MP_PREC_FP64 && precision != MP_PREC_FP32_REANCHOR)
+        return fail(ctx, MP_ERR_INVALID_ARG, "unknown precision %d", precision);
+    MP_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    ctx->launches = 0;
+    const bool a_dev = on_device(A);
+    const bool o_dev = on_device(dist2_out);
+    if (on_device(idx_out) != o_dev)
+        return fail(ctx, MP_ERR_INVALID_ARG, "dist2_out and idx_out live in different memory spaces");
+    const int64_t PL = S.PL, ndiag = S.hi - S.lo;
+
+    if (precision == MP_PREC_FP64) {
+        const int64_t B = blocklen > 0 ? blocklen : 500;
+        const int shards = fp64_shards(PL);
+        rc = reserve(ctx, fp64_scratch(n, m, ndiag, !o_dev));
+        if (rc) return rc;
+        Carve cv{(char*)ctx->arena};
+        double* Apad = cv.take<double>(n + 1);
+        double* cs = cv.take<double>(n);
+        double* cs2 = cv.take<double>(n);
+        double* muS = cv.take<double>(PL);
+        double* sInv = cv.take<double>(PL);
+        double* qt0 = cv.take<double>(ndiag);
+        double4* rec = cv.take<double4>(PL + kFp64Pad);
+        unsigned long long* kex = cv.take<unsigned long long>(PL * shards);
+        unsigned long long* kid = cv.take<unsigned long long>(PL * shards);
+        double* d2 = o_dev ? dist2_out : cv.take<double>(PL);
+        int64_t* ix = o_dev ? idx_out : cv.take<int64_t>(PL);
+
+        MP_CUDA(ctx, cudaMemcpyAsync(Apad, A, 8 * n, a_dev ? cudaMemcpyDeviceToDevice
+                                                           : cudaMemcpyHostToDevice, st));
+        mark(ctx, 0, st);
+        MP_CUDA(ctx, cudaMemsetAsync(Apad + n, 0, 8, st));
+        ref_prefix_kernel<<<1, 1, 0, st>>>(Apad, n, cs, cs2);
+        MP_LAUNCHED(ctx);
+        ref_stats_kernel<<<grid_for(PL), kThreads, 0, st>>>(cs, cs2, PL, m, muS, sInv);
+        MP_LAUNCHED(ctx);
+        if (ndiag > 0) {
+            first_qt_kernel<<<grid_for(ndiag), kThreads, 0, st>>>(Apad, m, S.lo, S.hi, qt0);
+            MP_LAUNCHED(ctx);
+        }
+        MP_CUDA(ctx, cudaMemsetAsync(rec + PL, 0, 32 * kFp64Pad, st));
+        pack_fp64_kernel<<<grid_for(PL), kThreads, 0, st>>>(Apad, m, PL, sInv, muS, rec);
+        MP_LAUNCHED(ctx);
+        MP_CUDA(ctx, cudaMemsetAsync(kex, 0, 8 * (size_t)PL * shards, st));
+        MP_CUDA(ctx, cudaMemsetAsync(kid, 0, 8 * (size_t)PL * shards, st));
+        mark(ctx, 1, st);
+        if (ndiag > 0) {
+            Fp64BandParams P{};
+            const int R = pick_fp64_R(ndiag);
+            P.colrec = rec;
+            P.rowrec = rec;
+            P.qt0 = qt0;
+            P.qt_out = nullptr;
+            P.g_lo = S.lo;
+            P.g_hi = S.hi;
+            P.nbands = (ndiag + 32 * R - 1) / (32 * R);
+            P.blk_origin = S.excl + 1;
+            P.B = B;
+            P.Tbase = PL;
+            P.kexact = kex;
+            P.kidx = kid;
+            P.key_stride = PL;
+            P.shards = shards;
+            P.m = (double)m;
+            P.floor = -1.0;
+            P.idx_bits = bits_for((uint64_t)PL);
+            launch_band(R, P, st);
+            MP_LAUNCHED(ctx);
+        }
+        mark(ctx, 2, st);
+        finalize_fp64_kernel<<<grid_for(PL), kThreads, 0, st>>>(kex, kid, PL, shards, PL, (double)m,
+                                                                bits_for((uint64_t)PL), d2, ix);
+        MP_LAUNCHED(ctx);
+        mark(ctx, 3, st);
+        if (!o_dev) {
+            MP_CUDA(ctx, cudaMemcpyAsync(dist2_out, d2, 8 * PL, cudaMemcpyDeviceToHost, st));
+            MP_CUDA(ctx, cudaMemcpyAsync(idx_out, ix, 8 * PL, cudaMemcpyDeviceToHost, st));
+        }
+        MP_CUDA(ctx, cudaStreamSynchronize(st));
+        collect_phases(ctx);
+        return MP_OK;
+    }
+
+    // ---- FP32 re-anchored form ----------------------------------------------
+    int64_t K = reanchor_k > 0 ? reanchor_k : 1024;
+    K = ((K + kFp32R - 1) / kFp32R) * kFp32R;
+    rc = reserve(ctx, fp32_scratch(n, m, !o_dev));
+    if (rc) return rc;
+    Carve cv{(char*)ctx->arena};
+    double* Apad = cv.take<double>(n + kFp32Pad);
+    int* nchg = cv.take<int>(n);
+    const int64_t nblk = (n + kThreads - 1) / kThreads;
+    int* tot = cv.take<int>(nblk + 1);
+    double* mean = cv.take<double>(PL + kFp32Pad);
+    double* norm = cv.take<double>(PL + kFp32Pad);
+    float4* rowrec = cv.take<float4>(2 * (PL + kFp32Pad));
+    float4* colrec = cv.take<float4>(2 * (PL + kFp32Pad));
+    unsigned long long* key = cv.take<unsigned long long>(PL);
+    double* d2 = o_dev ? dist2_out : cv.take<double>(PL);
+    int64_t* ix = o_dev ? idx_out : cv.take<int64_t>(PL);
+
+    MP_CUDA(ctx, cudaMemcpyAsync(Apad, A, 8 * n, a_dev ? cudaMemcpyDeviceToDevice
+                                                       : cudaMemcpyHostToDevice, st));
+    mark(ctx, 0, st);
+    MP_CUDA(ctx, cudaMemsetAsync(Apad + n, 0, 8 * kFp32Pad, st));
+    change_flags_kernel<<<grid_for(n), kThreads, 0, st>>>(Apad, n, nchg);
+    MP_LAUNCHED(ctx);
+    scan_blocks_kernel<<<(unsigned)nblk, kThreads, 0, st>>>(nchg, n, tot);
+    MP_LAUNCHED(ctx);
+    scan_totals_kernel<<<1, 1, 0, st>>>(tot, nblk);
+    MP_LAUNCHED(ctx);
+    scan_add_kernel<<<(unsigned)nblk, kThreads, 0, st>>>(nchg, n, tot);
+    MP_LAUNCHED(ctx);
+    MP_CUDA(ctx, cudaMemsetAsync(mean + PL, 0, 8 * kFp32Pad, st));
+    MP_CUDA(ctx, cudaMemsetAsync(norm + PL, 0, 8 * kFp32Pad, st));
+    const int64_t chunk = 256;
+    welford_kernel<<<grid_for((PL + chunk - 1) / chunk), kThreads, 0, st>>>(Apad, m, PL, chunk, nchg,
+                                                                           mean, norm);
+    MP_LAUNCHED(ctx);
+    pack_fp32_kernel<<<grid_for(PL + kFp32Pad), kThreads, 0, st>>>(
+        Apad, m, PL, kFp32R / 2, PL + kFp32Pad, mean, norm, rowrec, colrec);
+    MP_LAUNCHED(ctx);
+    const float ulim = (float)(1.0 + 1.0 / (double)m);
+    init_keys_kernel<<<grid_for(PL), kThreads, 0, st>>>(
+        key, PL, (unsigned long long)host_ord_f32(ulim) << 32);
+    MP_LAUNCHED(ctx);
+    mark(ctx, 1, st);
+    if (ndiag > 0) {
+        Fp32TileParams P{};
+        P.rowrec = rowrec;
+        P.colrec = colrec;
+        P.A = Apad;
+        P.mean = mean;
+        P.m = m;
+        P.PL = PL;
+        P.g_lo = S.lo;
+        P.g_hi = S.hi;
+        P.K = K;
+        const int64_t span = 32 * kFp32R;
+        P.nbands = (ndiag + span - 1) / span;
+        int64_t spp = 0;
+        const int64_t npairs = (P.nbands + 1) / 2;
+        for (int64_t p = 0; p < npairs; ++p) {
+            const int64_t l0 = PL - (S.lo + p * span);
+            int64_t t = (l0 + K - 1) / K;
+            const int64_t p2 = P.nbands - 1 - p;
+            if (p2 > p) t += (PL - (S.lo + p2 * span) + K - 1) / K;
+            spp = std::max(spp, t);
+        }
+        P.seg_per_pair = std::max<int64_t>(spp, 1);
+        P.key = key;
+        launch_fp32_tiles<kFp32R>(P, 0, npairs * P.seg_per_pair, st);
+        MP_LAUNCHED(ctx);
+    }
+    mark(ctx, 2, st);
+    finalize_fp32_kernel<<<grid_for(PL), kThreads, 0, st>>>(key, PL, (double)m, Apad, mean, norm, 0,
+                                                            d2, ix);
+    MP_LAUNCHED(ctx);
+    mark(ctx, 3, st);
+    if (!o_dev) {
+        MP_CUDA(ctx, cudaMemcpyAsync(dist2_out, d2, 8 * PL, cudaMemcpyDeviceToHost, st));
+        MP_CUDA(ctx, cudaMemcpyAsync(idx_out, ix, 8 * PL, cudaMemcpyDeviceToHost, st));
+    }
+    MP_CUDA(ctx, cudaStreamSynchronize(st));
+    collect_phases(ctx);
+    return MP_OK;
+}
+
+int mp_window_stats(mp_context* ctx, const double* A, int64_t n, int64_t m, double* muS_out,
+                    double* sInv_out, void* stream) {
+    if (!ctx) return MP_ERR_INVALID_ARG;
+    if (!A || !muS_out || !sInv_out) return fail(ctx, MP_ERR_INVALID_ARG, "null buffer");
+    if (m < 1 || n < m) return fail(ctx, MP_ERR_INVALID_ARG, "need 1 <= m <= n");
+    MP_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    ctx->launches = 0;
+    const int64_t PL = n - m + 1;
+    int rc = reserve(ctx, align_up(8 * n) * 3 + align_up(8 * PL) * 2 + 4096);
+    if (rc) return rc;
+    Carve cv{(char*)ctx->arena};
+    double* Ad = cv.take<double>(n);
+    double* cs = cv.take<double>(n);
+    double* cs2 = cv.take<double>(n);
+    double* mu = cv.take<double>(PL);
+    double* si = cv.take<double>(PL);
+    MP_CUDA(ctx, cudaMemcpyAsync(Ad, A, 8 * n, cudaMemcpyDefault, st));
+    ref_prefix_kernel<<<1, 1, 0, st>>>(Ad, n, cs, cs2);
+    MP_LAUNCHED(ctx);
+    ref_stats_kernel<<<grid_for(PL), kThreads, 0, st>>>(cs, cs2, PL, m, mu, si);
+    MP_LAUNCHED(ctx);
+    MP_CUDA(ctx, cudaMemcpyAsync(muS_out, mu, 8 * PL, cudaMemcpyDefault, st));
+    MP_CUDA(ctx, cudaMemcpyAsync(sInv_out, si, 8 * PL, cudaMemcpyDefault, st));
+    MP_CUDA(ctx, cudaStreamSynchronize(st));
+    return MP_OK;
+}
+
+int mp_first_qt(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t d_lo, int64_t d_hi,
+                double* qt, void* stream) {
+    if (!ctx) return MP_ERR_INVALID_ARG;
+    if (!A || !qt) return fail(ctx, MP_ERR_INVALID_ARG, "null buffer");
+    if (m < 1 || n < m || d_lo < 0 || d_hi > n - m + 1 || d_hi < d_lo)
+        return fail(ctx, MP_ERR_INVALID_ARG, "bad diagonal range");
+    MP_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    ctx->launches = 0;
+    const int64_t nd = d_hi - d_lo;
+    int rc = reserve(ctx, align_up(8 * n) + align_up(8 * std::max<int64_t>(nd, 1)) + 4096);
+    if (rc) return rc;
+    Carve cv{(char*)ctx->arena};
+    double* Ad = cv.take<double>(n);
+    double* q = cv.take<double>(nd);
+    MP_CUDA(ctx, cudaMemcpyAsync(Ad, A, 8 * n, cudaMemcpyDefault, st));
+    if (nd > 0) {
+        first_qt_kernel<<<grid_for(nd), kThreads, 0, st>>>(Ad, m, d_lo, d_hi, q);
+        MP_LAUNCHED(ctx);
+        MP_CUDA(ctx, cudaMemcpyAsync(qt, q, 8 * nd, cudaMemcpyDefault, st));
+    }
+    MP_CUDA(ctx, cudaStreamSynchronize(st));
+    return MP_OK;
+}
+
+int mp_eval_diag_block_triangle(mp_context* ctx, double* prof_colmin, int64_t* idx_colmin,
+                                double* prof_rowmin, int64_t* idx_rowmin, double* tmpQ,
+                                int64_t blocklen, int64_t trianglen, const double* A_hor,
+                                const double* A_vert, int64_t m, const double* s_hor,
+                                const double* mu_hor, const double* s_vert, const double* mu_vert,
+                                int64_t baserow, int64_t basecol, void* stream) {
+    if (!ctx) return MP_ERR_INVALID_ARG;
+    if (!prof_colmin || !idx_colmin || !prof_rowmin || !idx_rowmin || !tmpQ || !A_hor || !A_vert ||
+        !s_hor || !mu_hor || !s_vert || !mu_vert)
+        return fail(ctx, MP_ERR_INVALID_ARG, "null buffer");
+    if (blocklen < 1 || trianglen < 0 || m < 1 || baserow < 0 || basecol < 0)
+        return fail(ctx, MP_ERR_INVALID_ARG, "bad block geometry");
+    const int64_t T = trianglen;
+    if (T == 0) return MP_OK;
+    if (baserow + T >= (1ll << 31) || basecol + T >= (1ll << 31))
+        return fail(ctx, MP_ERR_NOT_SUPPORTED, "neighbour indices beyond 2^31");
+    MP_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    ctx->launches = 0;
+
+    // The two profile views: one region if they overlap, two otherwise.
+    const ptrdiff_t dp = prof_rowmin - prof_colmin;
+    const ptrdiff_t di = idx_rowmin - idx_colmin;
+    const bool overlap = (dp > -(ptrdiff_t)T && dp < (ptrdiff_t)T);
+    if (overlap && dp != di)
+        return fail(ctx, MP_ERR_INVALID_ARG, "aliased profile views need matching index views");
+    int64_t col_off, row_off, region;
+    double* region_p0 = nullptr;
+    int64_t* region_i0 = nullptr;
+    if (overlap) {
+        const int64_t lo = std::min<int64_t>(0, dp);
+        col_off = -lo;
+        row_off = dp - lo;
+        region = std::max<int64_t>(T, dp + T) - lo;
+        region_p0 = prof_colmin + lo;
+        region_i0 = idx_colmin + lo;
+    } else {
+        col_off = 0;
+        row_off = T;
+        region = 2 * T;
+    }
+    const int64_t nrec = T + kFp64Pad;
+    const int64_t nq = std::min<int64_t>(blocklen, T);
+    size_t need = 2 * align_up(32 * (size_t)nrec) + 2 * align_up(8 * (size_t)nq) +
+                  2 * align_up(8 * (size_t)region) * 2 + 2 * align_up(8 * (size_t)(T + m)) +
+                  4 * align_up(8 * (size_t)T) + 4096;
+    int rc = reserve(ctx, need);
+    if (rc) return rc;
+    Carve cv{(char*)ctx->arena};
+    double4* colrec = cv.take<double4>(nrec);
+    double4* rowrec = cv.take<double4>(nrec);
+    double* q = cv.take<double>(nq);
+    double* qout = cv.take<double>(nq);
+    double* prof = cv.take<double>(region);
+    int64_t* pidx = cv.take<int64_t>(region);
+    unsigned long long* kex = cv.take<unsigned long long>(region);
+    unsigned long long* kid = cv.take<unsigned long long>(region);
+    double* ah = cv.take<double>(T + m);
+    double* av = cv.take<double>(T + m);
+    double* sh = cv.take<double>(T);
+    double* mh = cv.take<double>(T);
+    double* sv = cv.take<double>(T);
+    double* mv = cv.take<double>(T);
+    const cudaMemcpyKind K = cudaMemcpyDefault;
+    MP_CUDA(ctx, cudaMemcpyAsync(ah, A_hor, 8 * (T + m), K, st));
+    MP_CUDA(ctx, cudaMemcpyAsync(av, A_vert, 8 * (T + m), K, st));
+    MP_CUDA(ctx, cudaMemcpyAsync(sh, s_hor, 8 * T, K, st));
+    MP_CUDA(ctx, cudaMemcpyAsync(mh, mu_hor, 8 * T, K, st));
+    MP_CUDA(ctx, cudaMemcpyAsync(sv, s_vert, 8 * T, K, st));
+    MP_CUDA(ctx, cudaMemcpyAsync(mv, mu_vert, 8 * T, K, st));
+    MP_CUDA(ctx, cudaMemcpyAsync(q, tmpQ, 8 * nq, K, st));
+    if (overlap) {
+        MP_CUDA(ctx, cudaMemcpyAsync(prof, region_p0, 8 * region, K, st));
+        MP_CUDA(ctx, cudaMemcpyAsync(pidx, region_i0, 8 * region, K, st));
+    } else {
+        MP_CUDA(ctx, cudaMemcpyAsync(prof, prof_colmin, 8 * T, K, st));
+        MP_CUDA(ctx, cudaMemcpyAsync(pidx, idx_colmin, 8 * T, K, st));
+        MP_CUDA(ctx, cudaMemcpyAsync(prof + T, prof_rowmin, 8 * T, K, st));
+        MP_CUDA(ctx, cudaMemcpyAsync(pidx + T, idx_rowmin, 8 * T, K, st));
+    }
+    MP_CUDA(ctx, cudaMemsetAsync(colrec + T, 0, 32 * kFp64Pad, st));
+    MP_CUDA(ctx, cudaMemsetAsync(rowrec + T, 0, 32 * kFp64Pad, st));
+    pack_fp64_kernel<<<grid_for(T), kThreads, 0, st>>>(ah, m, T, sh, mh, colrec);
+    MP_LAUNCHED(ctx);
+    pack_fp64_kernel<<<grid_for(T), kThreads, 0, st>>>(av, m, T, sv, mv, rowrec);
+    MP_LAUNCHED(ctx);
+    block_keys_init_kernel<<<grid_for(region), kThreads, 0, st>>>(prof, region, kex, kid);
+    MP_LAUNCHED(ctx);
+
+    Fp64BandParams P{};
+    const int R = pick_fp64_R(nq);
+    P.colrec = colrec;
+    P.rowrec = rowrec;
+    P.qt0 = q;
+    P.qt_out = qout;
+    P.g_lo = 0;
+    P.g_hi = nq;
+    P.nbands = (nq + 32 * R - 1) / (32 * R);
+    P.blk_origin = 0;
+    P.B = blocklen;
+    P.Tbase = T;
+    P.kexact = kex;
+    P.kidx = kid;
+    P.key_stride = region;
+    P.shards = 1;
+    P.row_key_off = row_off;
+    P.col_key_off = col_off;
+    P.row_nb_off = baserow;
+    P.col_nb_off = basecol;
+    P.m = (double)m;
+    P.floor = -1.7976931348623157e308;
+    const int ib = bits_for((uint64_t)std::max(baserow + T, basecol + T));
+    P.idx_bits = ib;
+    launch_band(R, P, st);
+    MP_LAUNCHED(ctx);
+    block_finalize_kernel<<<grid_for(region), kThreads, 0, st>>>(kex, kid, region, 1, region, ib,
+                                                                 prof, pidx);
+    MP_LAUNCHED(ctx);
+    MP_CUDA(ctx, cudaMemcpyAsync(tmpQ, qout, 8 * nq, K, st));
+    if (overlap) {
+        MP_CUDA(ctx, cudaMemcpyAsync(region_p0, prof, 8 * region, K, st));
+        MP_CUDA(ctx, cudaMemcpyAsync(region_i0, pidx, 8 * region, K, st));
+    } else {
+        MP_CUDA(ctx, cudaMemcpyAsync(prof_colmin, prof, 8 * T, K, st));
+        MP_CUDA(ctx, cudaMemcpyAsync(idx_colmin, pidx, 8 * T, K, st));
+        MP_CUDA(ctx, cudaMemcpyAsync(prof_rowmin, prof + T, 8 * T, K, st));
+        MP_CUDA(ctx, cudaMemcpyAsync(idx_rowmin, pidx + T, 8 * T, K, st));
+    }
+    MP_CUDA(ctx, cudaStreamSynchronize(st));
+    return MP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,251 @@
+// FP64 diagonal-band join: the reference's SCRIMP recurrence evaluated with
+// the reference's own per-cell arithmetic, one warp per band of 32*R
+// adjacent diagonals.
+//
+// Reference: eval_diag_block_triangle, AVX2 branch
+// (scrimppp/src/kernels.cpp:170-307), driven over blocks of blocklen
+// diagonals by ScrimpVertBlocked (scrimppp/src/ScrimpVertBlocked.cpp:139-168).
+// Per cell (column j, diagonal g, row r = j + g):
+//   4-wide part : score = fma(QT, s_r*s_j, -(mu_j*mu_r))
+//                 QT    = fma(-A[r], A[j], fma(A[r+m], A[j+m], QT))
+//   remainder   : score = QT*(s_r*s_j) - mu_r*mu_j, QT = (QT + A[r+m]*A[j+m]) - A[r]*A[j]
+// (every product and sum separately rounded).  A cell is in the remainder
+// iff its offset in the reference block, delta, is >= 4*floor(cnt/4) with
+// cnt = min(blocklen, T - j); for a diagonal that is only its last
+// 3 - delta%4 cells (or all of it when delta >= blocklen & ~3).
+//
+// Work layout (B200): lane l of a warp owns diagonals g0 + a, a < R,
+// g0 = band start + l*R; all lanes walk the same column j.  Per step a lane
+// evaluates R cells: the column maximum over the warp comes from two warp
+// reductions (high, then low word of the ordered score), the row maxima
+// accumulate in registers for R steps and then pass through a per-warp shared
+// memory ring (one writer per slot per chunk, no atomics) until the warp's
+// lowest lane has seen the row.  Finished rows and columns go to global
+// memory as 64-bit max reductions into one of several key shards.  Bands are
+// paired (k, nbands-1-k) per warp so every warp does the same work
+// (the reference's triv_par balance rule, ScrimpTrivialPar.cpp:200-224).
+#include <float.h>
+
+#include "mp_common.cuh"
+#include "mp_kernels.h"
+
+namespace mpgpu {
+
+namespace {
+
+// 32-byte record through the read-only path as two 16-byte loads.
+__device__ __forceinline__ double4 ld_rec(const double4* p) {
+    const double2 lo = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 hi = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+
+__device__ __forceinline__ void flush_fp64(const Fp64BandParams& P, int shard, int64_t slot,
+                                           double score, int64_t neighbour) {
+    unsigned long long* ke = P.kexact + (int64_t)shard * P.key_stride + slot;
+    unsigned long long* ki = P.kidx + (int64_t)shard * P.key_stride + slot;
+    atomicMax(ke, ord_f64(score));
+    atomicMax(ki, idx_key_f64(score, P.m, (unsigned long long)neighbour, P.idx_bits));
+}
+
+template <int R, bool FAST>
+__device__ __forceinline__ void chunk_fp64(const Fp64BandParams& P, int64_t jc, const double4* rowp,
+                                           double4 (&rwin)[R], double (&qt)[R],
+                                           const int64_t (&len)[R], const int64_t (&psw)[R],
+                                           double (&acc_s)[2 * R - 1], int (&acc_a)[2 * R - 1],
+                                           int64_t g0, int lane, int shard) {
+#pragma unroll
+    for (int b = 0; b < R; ++b) {
+        const int64_t j = jc + b;
+        rwin[(b + R - 1) % R] = ld_rec(rowp + jc + b + R - 1);
+        const double4 cv = ld_rec(P.colrec + j);
+        double cbest = -DBL_MAX;
+        int ca = 0;
+#pragma unroll
+        for (int a = 0; a < R; ++a) {
+            const double4 rv = rwin[(b + a) % R];
+            double score;
+            if (FAST) {
+                // 4-wide part of the reference kernel (kernels.cpp:206-225)
+                const double ss = __dmul_rn(rv.z, cv.z);
+                const double mm = __dmul_rn(cv.w, rv.w);
+                score = __fma_rn(qt[a], ss, -mm);
+                qt[a] = __fma_rn(-rv.x, cv.x, __fma_rn(rv.y, cv.y, qt[a]));
+            } else if (j < len[a]) {
+                const double ss = __dmul_rn(rv.z, cv.z);
+                if (j <= psw[a]) {
+                    const double mm = __dmul_rn(cv.w, rv.w);
+                    score = __fma_rn(qt[a], ss, -mm);
+                    qt[a] = __fma_rn(-rv.x, cv.x, __fma_rn(rv.y, cv.y, qt[a]));
+                } else {
+                    // scalar remainder (kernels.cpp:282-289), no fusion
+                    score = __dsub_rn(__dmul_rn(qt[a], ss), __dmul_rn(rv.w, cv.w));
+                    qt[a] = __dsub_rn(__dadd_rn(qt[a], __dmul_rn(rv.y, cv.y)),
+                                      __dmul_rn(rv.x, cv.x));
+                }
+            } else {
+                score = -DBL_MAX;
+            }
+            if (score > acc_s[b + a]) {
+                acc_s[b + a] = score;
+                acc_a[b + a] = a;
+            }
+            if (score > cbest) {
+                cbest = score;
+                ca = a;
+            }
+        }
+        // column j: warp maximum of the lanes' bests, by ordered key
+        const unsigned long long key = (cbest > P.floor) ? ord_f64(cbest) : 0ull;
+        const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+        const unsigned mhi = __reduce_max_sync(kFullMask, hi);
+        if (mhi != 0u) {
+            const unsigned mlo = __reduce_max_sync(kFullMask, hi == mhi ? lo : 0u);
+            const unsigned win = __ballot_sync(kFullMask, hi == mhi && lo == mlo);
+            if (lane == __ffs(win) - 1)
+                flush_fp64(P, shard, j + P.col_key_off, cbest, j + g0 + ca + P.row_nb_off);
+        }
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band, int lane,
+                                          int shard, double* ring_s, int* ring_c) {
+    constexpr int RING = 32 * R;
+    const int64_t gb = P.g_lo + band * (int64_t)RING;
+    const int64_t g0 = gb + (int64_t)lane * R;
+    const int64_t jmax = P.Tbase - gb;  // length of the band's longest diagonal
+    if (jmax <= 0) return;
+
+    double qt[R];
+    int64_t len[R], psw[R];
+    int64_t minpsw = INT64_MAX;
+#pragma unroll
+    for (int a = 0; a < R; ++a) {
+        const int64_t g = g0 + a;
+        if (g < P.g_hi) {
+            const int64_t delta = (g - P.blk_origin) % P.B;
+            const int64_t T = P.Tbase - (g - delta);
+            qt[a] = P.qt0[g - P.g_lo];
+            len[a] = T - delta;
+            psw[a] = (delta < (P.B & ~3ll)) ? T - 4 * (delta / 4 + 1) : -1;
+        } else {
+            qt[a] = 0.0;
+            len[a] = 0;
+            psw[a] = -1;
+        }
+        minpsw = min(minpsw, psw[a]);
+    }
+
+    // ring of row partials, slot = (r - gb) mod RING
+    for (int k = lane; k < RING; k += 32) {
+        ring_s[k] = -DBL_MAX;
+        ring_c[k] = 0;
+    }
+    __syncwarp();
+
+    double acc_s[2 * R - 1];
+    int acc_a[2 * R - 1];
+#pragma unroll
+    for (int k = 0; k < 2 * R - 1; ++k) {
+        acc_s[k] = -DBL_MAX;
+        acc_a[k] = 0;
+    }
+
+    // register window of row records: slot (k mod R) holds row g0 + jc + k
+    double4 rwin[R];
+    const double4* rowp = P.rowrec + g0;
+#pragma unroll
+    for (int k = 0; k < R - 1; ++k) rwin[k] = ld_rec(rowp + k);
+
+    for (int64_t jc = 0; jc < jmax; jc += R) {
+        const bool fast = __all_sync(kFullMask, jc + R - 1 <= minpsw);
+        if (fast)
+            chunk_fp64<R, true>(P, jc, rowp, rwin, qt, len, psw, acc_s, acc_a, g0, lane, shard);
+        else
+            chunk_fp64<R, false>(P, jc, rowp, rwin, qt, len, psw, acc_s, acc_a, g0, lane, shard);
+        // rows jc + g0 + [0, R) are done for this lane: merge into the ring
+        const int base = (int)(((jc / R) + lane) % 32) * R;
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            if (acc_s[k] > ring_s[base + k]) {
+                ring_s[base + k] = acc_s[k];
+                ring_c[base + k] = (int)(jc + k - acc_a[k]);
+            }
+        }
+        __syncwarp();
+        // rows jc + gb + [0, R) have now met every lane: flush and free
+        if (lane < R) {
+            const int e = (int)((jc / R) % 32) * R + lane;
+            const double s = ring_s[e];
+            if (s > P.floor) flush_fp64(P, shard, jc + gb + lane + P.row_key_off, s,
+                                     ring_c[e] + P.col_nb_off);
+            ring_s[e] = -DBL_MAX;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < R - 1; ++k) {
+            acc_s[k] = acc_s[k + R];
+            acc_a[k] = acc_a[k + R];
+        }
+#pragma unroll
+        for (int k = R - 1; k < 2 * R - 1; ++k) acc_s[k] = -DBL_MAX;
+    }
+
+    // drain: carried rows jend + g0 + [0, R-1) into the ring, then every slot
+    const int64_t jend = ((jmax + R - 1) / R) * R;
+    const int base = (int)(((jend / R) + lane) % 32) * R;
+#pragma unroll
+    for (int k = 0; k < R - 1; ++k) {
+        if (acc_s[k] > ring_s[base + k]) {
+            ring_s[base + k] = acc_s[k];
+            ring_c[base + k] = (int)(jend + k - acc_a[k]);
+        }
+    }
+    __syncwarp();
+    for (int e = lane; e < RING; e += 32) {
+        const double s = ring_s[e];
+        if (s > P.floor) {
+            const int64_t rel = ((int64_t)e - jend % RING + RING) % RING;
+            flush_fp64(P, shard, jend + gb + rel + P.row_key_off, s, ring_c[e] + P.col_nb_off);
+        }
+    }
+    __syncwarp();
+
+    if (P.qt_out) {
+#pragma unroll
+        for (int a = 0; a < R; ++a)
+            if (g0 + a < P.g_hi) P.qt_out[g0 + a - P.g_lo] = qt[a];
+    }
+}
+
+template <int R>
+__global__ void __launch_bounds__(32 * kFp64WarpsPerBlock) fp64_band_kernel(const Fp64BandParams P) {
+    __shared__ double ring_s_all[kFp64WarpsPerBlock][32 * R];
+    __shared__ int ring_c_all[kFp64WarpsPerBlock][32 * R];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const int64_t job = (int64_t)blockIdx.x * kFp64WarpsPerBlock + w;
+    const int64_t njobs = (P.nbands + 1) / 2;
+    if (job >= njobs) return;
+    const int shard = (int)(job % P.shards);
+    band_fp64<R>(P, job, lane, shard, ring_s_all[w], ring_c_all[w]);
+    const int64_t partner = P.nbands - 1 - job;
+    if (partner > job) band_fp64<R>(P, partner, lane, shard, ring_s_all[w], ring_c_all[w]);
+}
+
+}  // namespace
+
+template <int R>
+void launch_fp64_band(const Fp64BandParams& P, cudaStream_t s) {
+    const int64_t njobs = (P.nbands + 1) / 2;
+    const int64_t blocks = (njobs + kFp64WarpsPerBlock - 1) / kFp64WarpsPerBlock;
+    if (blocks > 0) fp64_band_kernel<R><<<(unsigned)blocks, 32 * kFp64WarpsPerBlock, 0, s>>>(P);
+}
+
+template void launch_fp64_band<1>(const Fp64BandParams&, cudaStream_t);
+template void launch_fp64_band<2>(const Fp64BandParams&, cudaStream_t);
+template void launch_fp64_band<4>(const Fp64BandParams&, cudaStream_t);
+template void launch_fp64_band<8>(const Fp64BandParams&, cudaStream_t);
+
+}  // namespace mpgpu

@@ -1,0 +1,84 @@
+// Kernel declarations and launch parameter blocks shared by the mpgpu
+// translation units (device code and the C-ABI layer).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mpgpu {
+
+// ---- preparation (mp_prep.cu) ----------------------------------------------
+__global__ void ref_prefix_kernel(const double* A, int64_t n, double* cs, double* cs2);
+__global__ void ref_stats_kernel(const double* cs, const double* cs2, int64_t PL, int64_t m,
+                                 double* muS, double* sInv);
+__global__ void first_qt_kernel(const double* A, int64_t m, int64_t d_lo, int64_t d_hi,
+                                double* qt);
+__global__ void pack_fp64_kernel(const double* Apad, int64_t m, int64_t count, const double* sInv,
+                                 const double* muS, double4* rec);
+__global__ void change_flags_kernel(const double* A, int64_t n, int* chg);
+__global__ void scan_blocks_kernel(int* x, int64_t n, int* block_tot);
+__global__ void scan_totals_kernel(int* tot, int64_t nblocks);
+__global__ void scan_add_kernel(int* x, int64_t n, const int* tot);
+__global__ void welford_kernel(const double* A, int64_t m, int64_t PL, int64_t chunk,
+                               const int* nchg, double* mean_out, double* norm_out);
+__global__ void pack_fp32_kernel(const double* A, int64_t m, int64_t PL, int H, int64_t count,
+                                 const double* mean, const double* norm, float4* rowrec,
+                                 float4* colrec);
+
+// ---- FP64 diagonal-band join (mp_join_fp64.cu) ------------------------------
+// Diagonal g (g_lo <= g < g_hi) meets column j in row r = j + g, for
+// j < Tbase - g.  The reference's block geometry (blocks of B diagonals
+// starting at blk_origin, triangle length T = Tbase - block start) decides
+// per cell whether the fused or the separately rounded arithmetic applies.
+struct Fp64BandParams {
+    const double4* colrec;  // colrec[j] = {A_hor[j], A_hor[j+m], s_hor[j], mu_hor[j]}
+    const double4* rowrec;  // rowrec[r] = {A_vert[r], A_vert[r+m], s_vert[r], mu_vert[r]}
+    const double* qt0;      // qt0[g - g_lo]: running dot product at j = 0
+    double* qt_out;         // optional: dot product after the last cell, per diagonal
+    int64_t g_lo, g_hi, nbands;
+    int64_t blk_origin, B, Tbase;
+    unsigned long long* kexact;  // [shards][key_stride] ordered score, max-merged
+    unsigned long long* kidx;    // [shards][key_stride] truncated score | neighbour
+    int64_t key_stride;
+    int shards;
+    int64_t row_key_off, col_key_off;  // key slot of row r / column j
+    int64_t row_nb_off, col_nb_off;    // neighbour written for column j / row r
+    double m;
+    double floor;  // only scores strictly above it are merged (-1: reference init)
+    int idx_bits;
+};
+constexpr int kFp64WarpsPerBlock = 4;
+template <int R>
+void launch_fp64_band(const Fp64BandParams& P, cudaStream_t s);
+
+// ---- FP32 re-anchored tile join (mp_join_fp32.cu) ---------------------------
+struct Fp32TileParams {
+    const float4* rowrec;  // pairs (x[j], x[j+H]) of df, dg, nn; 2 float4 per row
+    const float4* colrec;  // duplicated, negated column terms; 2 float4 per column
+    const double* A;       // series (FP64) for the anchors
+    const double* mean;    // window means (FP64)
+    int64_t m, PL;
+    int64_t g_lo, g_hi;    // diagonals evaluated
+    int64_t K;             // columns per tile = re-anchor interval
+    int64_t nbands;        // bands of 32R diagonals
+    int64_t seg_per_pair;  // tiles per band pair (k, nbands-1-k), max over pairs
+    unsigned long long* key;  // [PL] (ordered u << 32 | neighbour), min-merged
+};
+template <int R>
+void launch_fp32_tiles(const Fp32TileParams& P, int64_t first_tile, int64_t count, cudaStream_t s);
+
+// ---- finalisation (mp_finalize.cu) -------------------------------------------
+__global__ void init_keys_kernel(unsigned long long* k, int64_t count, unsigned long long v);
+__global__ void finalize_fp64_kernel(const unsigned long long* kexact, const unsigned long long* kidx,
+                                     int64_t key_stride, int shards, int64_t PL, double m,
+                                     int idx_bits, double* d2, int64_t* idx);
+__global__ void finalize_fp32_kernel(const unsigned long long* key, int64_t PL, double m,
+                                     const double* A, const double* mean, const double* norm,
+                                     int refine, double* d2, int64_t* idx);
+__global__ void block_keys_init_kernel(const double* prof, int64_t count, unsigned long long* kexact,
+                                       unsigned long long* kidx);
+__global__ void block_finalize_kernel(const unsigned long long* kexact, const unsigned long long* kidx,
+                                      int64_t key_stride, int shards, int64_t count, int idx_bits,
+                                      double* prof, int64_t* idx);
+
+}  // namespace mpgpu

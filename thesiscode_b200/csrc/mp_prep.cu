@@ -1,0 +1,233 @@
+// Per-window preparation kernels: window statistics, first dot products and
+// the packed row/column records the join kernels stream.
+//
+// Two statistics paths:
+//  * reference-exact (FP64 form): the reference's prefix-sum formula,
+//    scrimppp/src/ScrimpSequOpt.cpp:33-79, evaluated with explicitly rounded
+//    operations (__dadd_rn/__dmul_rn/... are never contracted into FMAs) so the
+//    result is bit-identical to the reference built with IEEE semantics.  The
+//    prefix sums are a dependent chain and run on one thread.
+//  * FP64 Welford (FP32 form): each thread slides Welford's mean/M2 update
+//    over a chunk of windows, restarting from a fresh Welford pass at every
+//    chunk start; exact zero-variance windows are found with an integer count
+//    of value changes, so a constant window at any level is flagged exactly.
+#include "mp_common.cuh"
+#include "mp_kernels.h"
+
+namespace mpgpu {
+
+// ---- reference-exact statistics -------------------------------------------
+
+// cs[i] = A[i] + cs[i-1], cs2[i] = A[i]*A[i] + cs2[i-1] in index order
+// (ScrimpSequOpt.cpp:43-49).  One thread: the chain is inherently serial.
+__global__ void ref_prefix_kernel(const double* __restrict__ A, int64_t n, double* __restrict__ cs,
+                                  double* __restrict__ cs2) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double s = A[0];
+    double s2 = __dmul_rn(A[0], A[0]);
+    cs[0] = s;
+    cs2[0] = s2;
+    int64_t i = 1;
+    for (; i + 8 <= n; i += 8) {
+        double a[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = __ldg(A + i + k);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            s = __dadd_rn(a[k], s);
+            s2 = __dadd_rn(__dmul_rn(a[k], a[k]), s2);
+            cs[i + k] = s;
+            cs2[i + k] = s2;
+        }
+    }
+    for (; i < n; ++i) {
+        const double a = A[i];
+        s = __dadd_rn(a, s);
+        s2 = __dadd_rn(__dmul_rn(a, a), s2);
+        cs[i] = s;
+        cs2[i] = s2;
+    }
+}
+
+// Window sums from prefix differences, mean = S/m, var = S2/m - mean^2,
+// sInv = 1/sqrt(var), muS = (mean*sInv)*sqrt(m) (ScrimpSequOpt.cpp:50-68).
+__global__ void ref_stats_kernel(const double* __restrict__ cs, const double* __restrict__ cs2,
+                                 int64_t PL, int64_t m, double* __restrict__ muS,
+                                 double* __restrict__ sInv) {
+    const double dm = (double)m;
+    const double sqrt_m = __dsqrt_rn(dm);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < PL;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double s = (i == 0) ? cs[m - 1] : __dsub_rn(cs[m - 1 + i], cs[i - 1]);
+        const double s2 = (i == 0) ? cs2[m - 1] : __dsub_rn(cs2[m - 1 + i], cs2[i - 1]);
+        const double mean = __ddiv_rn(s, dm);
+        const double var = __dsub_rn(__ddiv_rn(s2, dm), __dmul_rn(mean, mean));
+        const double si = __ddiv_rn(1.0, __dsqrt_rn(var));
+        sInv[i] = si;
+        muS[i] = __dmul_rn(__dmul_rn(mean, si), sqrt_m);
+    }
+}
+
+// First dot product per diagonal, summed in k order without fusion
+// (ScrimpSequOpt.cpp:81-96).  Consecutive threads take consecutive diagonals
+// so the A[k+d] reads coalesce and A[k] is a broadcast.
+__global__ void first_qt_kernel(const double* __restrict__ A, int64_t m, int64_t d_lo,
+                                int64_t d_hi, double* __restrict__ qt) {
+    for (int64_t d = d_lo + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; d < d_hi;
+         d += (int64_t)gridDim.x * blockDim.x) {
+        double z = 0.0;
+        const double* a = A + d;
+        for (int64_t k = 0; k < m; ++k) z = __dadd_rn(z, __dmul_rn(__ldg(a + k), __ldg(A + k)));
+        qt[d - d_lo] = z;
+    }
+}
+
+// Row/column record of the FP64 join: {A[i], A[i+m], sInv[i], muS[i]}.
+// `Apad` holds n+1 values (A[n] = 0 feeds only the update after a diagonal's
+// last cell, whose result is never used).
+__global__ void pack_fp64_kernel(const double* __restrict__ Apad, int64_t m, int64_t count,
+                                 const double* __restrict__ sInv, const double* __restrict__ muS,
+                                 double4* __restrict__ rec) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        rec[i] = make_double4(Apad[i], Apad[i + m], sInv[i], muS[i]);
+    }
+}
+
+// ---- FP64 Welford statistics (FP32 form) ----------------------------------
+
+// chg[i] = 1 if A[i] != A[i-1] (i >= 1), chg[0] = 0; an inclusive scan of chg
+// gives the number of value changes up to i.
+__global__ void change_flags_kernel(const double* __restrict__ A, int64_t n, int* __restrict__ chg) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        chg[i] = (i > 0 && A[i] != A[i - 1]) ? 1 : 0;
+}
+
+// Block-level inclusive scan helper (Hillis-Steele over a warp, then warps).
+__device__ __forceinline__ int warp_incl_scan(int v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kFullMask, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Two-level inclusive scan of int flags: per-block scan + block totals.
+__global__ void scan_blocks_kernel(int* __restrict__ x, int64_t n, int* __restrict__ block_tot) {
+    __shared__ int wsum[32];
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int v = (i < n) ? x[i] : 0;
+    v = warp_incl_scan(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 31) wsum[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        int t = (lane < (int)(blockDim.x >> 5)) ? wsum[lane] : 0;
+        t = warp_incl_scan(t);
+        wsum[lane] = t;
+    }
+    __syncthreads();
+    if (w > 0) v += wsum[w - 1];
+    if (i < n) x[i] = v;
+    if (threadIdx.x == blockDim.x - 1) block_tot[blockIdx.x] = v;
+}
+
+__global__ void scan_totals_kernel(int* __restrict__ tot, int64_t nblocks) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    int s = 0;
+    for (int64_t b = 0; b < nblocks; ++b) {
+        s += tot[b];
+        tot[b] = s;
+    }
+}
+
+__global__ void scan_add_kernel(int* __restrict__ x, int64_t n, const int* __restrict__ tot) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n && blockIdx.x > 0) x[i] += tot[blockIdx.x - 1];
+}
+
+// Welford over a chunk of `chunk` consecutive windows per thread: a full
+// Welford pass for the first window, then the sliding update
+//   mean' = mean + (x_in - x_out)/m
+//   M2'   = M2 + (x_in - x_out)*(x_in - mean' + x_out - mean).
+// Outputs mean (FP64) and norm = 1/sqrt(M2) (FP64; NaN for a window whose
+// values are all equal, so every correlation with it is NaN).
+__global__ void welford_kernel(const double* __restrict__ A, int64_t m, int64_t PL, int64_t chunk,
+                               const int* __restrict__ nchg, double* __restrict__ mean_out,
+                               double* __restrict__ norm_out) {
+    const int64_t nthreads = (PL + chunk - 1) / chunk;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nthreads;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i0 = t * chunk;
+        const int64_t i1 = min(PL, i0 + chunk);
+        double mean = 0.0, M2 = 0.0;
+        for (int64_t k = 0; k < m; ++k) {
+            const double x = A[i0 + k];
+            const double delta = x - mean;
+            mean += delta / (double)(k + 1);
+            M2 += delta * (x - mean);
+        }
+        const double inv_m = 1.0 / (double)m;
+        for (int64_t i = i0; i < i1; ++i) {
+            if (i > i0) {
+                const double xin = A[i + m - 1], xout = A[i - 1];
+                const double mnew = mean + (xin - xout) * inv_m;
+                M2 += (xin - xout) * (xin - mnew + xout - mean);
+                mean = mnew;
+            }
+            const bool flat = (nchg[i + m - 1] - nchg[i]) == 0;
+            mean_out[i] = mean;
+            norm_out[i] = (flat || !(M2 > 0.0)) ? __longlong_as_double(0x7ff8000000000000ll)
+                                                : 1.0 / sqrt(M2);
+        }
+    }
+}
+
+// FP32 records.  For window i (i < PL):
+//   df[i] = (A[i+m] - A[i]) / 2,  dg[i] = (A[i+m] - mean[i+1]) + (A[i] - mean[i])
+// (zero for the last window, whose successor does not exist), nn[i] = norm[i].
+// Row records are stored as pairs (x[j], x[j+H]) for the f32x2 datapath:
+//   rowrec[j] = {df[j], df[j+H], dg[j], dg[j+H], nn[j], nn[j+H], 0, 0}
+// Column records duplicate and negate the column terms:
+//   colrec[p] = {-df[p], -df[p], -dg[p], -dg[p], nn[p], nn[p], 0, 0}
+// Entries past PL read as df = dg = 0, nn = NaN.
+__device__ __forceinline__ void fp32_terms(const double* A, int64_t m, int64_t PL,
+                                           const double* mean, const double* norm, int64_t i,
+                                           float& df, float& dg, float& nn) {
+    if (i >= PL) {
+        df = 0.f;
+        dg = 0.f;
+        nn = __int_as_float(0x7fffffff);
+        return;
+    }
+    if (i + 1 < PL) {
+        const double xin = A[i + m], xout = A[i];
+        df = (float)((xin - xout) * 0.5);
+        dg = (float)((xin - mean[i + 1]) + (xout - mean[i]));
+    } else {
+        df = 0.f;
+        dg = 0.f;
+    }
+    nn = (float)norm[i];
+}
+
+__global__ void pack_fp32_kernel(const double* __restrict__ A, int64_t m, int64_t PL, int H,
+                                 int64_t count, const double* __restrict__ mean,
+                                 const double* __restrict__ norm, float4* __restrict__ rowrec,
+                                 float4* __restrict__ colrec) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < count;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        float df0, dg0, nn0, df1, dg1, nn1;
+        fp32_terms(A, m, PL, mean, norm, j, df0, dg0, nn0);
+        fp32_terms(A, m, PL, mean, norm, j + H, df1, dg1, nn1);
+        rowrec[2 * j] = make_float4(df0, df1, dg0, dg1);
+        rowrec[2 * j + 1] = make_float4(nn0, nn1, 0.f, 0.f);
+        colrec[2 * j] = make_float4(-df0, -df0, -dg0, -dg0);
+        colrec[2 * j + 1] = make_float4(nn0, nn0, 0.f, 0.f);
+    }
+}
+
+}  // namespace mpgpu
