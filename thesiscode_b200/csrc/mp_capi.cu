@@ -123,20 +123,24 @@ unsigned host_ord_f32(float v) {
     return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
 }
 
+// Key shards spread the 64-bit max reductions of concurrently running bands
+// (which all walk the same columns) over more addresses; kept small enough
+// (~32 MB of keys) to stay resident in L2.
 int fp64_shards(int64_t PL) {
     const double per = 16.0 * (double)PL;
-    int64_t s = (int64_t)(4.0e9 / per);
-    return (int)std::max<int64_t>(1, std::min<int64_t>(32, s));
+    int64_t s = (int64_t)(32.0e6 / per);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(16, s));
 }
 
-// Warps in flight wanted per launch: 148 SMs x 12 resident warps.
+// Diagonals per lane: 8 amortises the per-column warp reduction best; fewer
+// only when the band count would leave SMs idle (>= 4 warps per SM wanted).
 int pick_fp64_R(int64_t ndiag) {
-    const int64_t want = 148 * 12;
-    for (int R : {8, 4, 2}) {
+    for (int R : {8, 4}) {
         const int64_t nb = (ndiag + 32 * R - 1) / (32 * R);
-        if ((nb + 1) / 2 >= want) return R;
+        if ((nb + 1) / 2 >= 148 * 4) return R;
     }
-    return 1;
+    const int64_t nb2 = (ndiag + 63) / 64;
+    return (nb2 + 1) / 2 >= 148 ? 2 : 1;
 }
 
 int launch_band(int R, const Fp64BandParams& P, cudaStream_t s) {

@@ -79,7 +79,42 @@ __device__ __forceinline__ float fmin3(float a, float b, float c) {
     return d;
 }
 
-// Bounded-work guard: device loops that wait on nothing but their own data
-// need no limit; this library has no cross-CTA waits at all.
+// ---------------------------------------------------------------------------
+// Per-warp ring of 32-byte row records in shared memory.
+//
+// Lane l of a band reads record base + 8*l + k while the other lanes read
+// theirs, i.e. 32 records 8 apart.  Read straight from global memory those hit
+// 32 cache lines per instruction; staged here they come in with coalesced
+// 16-byte loads and go out conflict-free: slot s lives at byte
+//   off(s) = 32*s + 16*(s >> 3),
+// a 16-byte gap after every 8 records, so the eight lanes of a quarter-warp
+// (records 8 apart, 272 bytes apart) start in eight distinct 16-byte bank
+// groups (a wrap moves a slot by 320 records = 680 chunks, a multiple of 8,
+// so it keeps its group).  Slots 320..327 mirror slots 0..7, so the 8
+// consecutive records a lane reads in one chunk never wrap: their offsets are
+// the chunk's base plus compile-time constants.
+// ---------------------------------------------------------------------------
+constexpr int kRecRing = 320;  // records per warp ring (multiple of 8, >= 33*8 + 16)
+constexpr int kRecMirror = 8;
+constexpr int kRecRingBytes = 32 * (kRecRing + kRecMirror) + 16 * ((kRecRing + kRecMirror) / 8);
+
+__device__ __forceinline__ int rec_off(int slot) { return 32 * slot + 16 * (slot >> 3); }
+
+// Offset of record (s0 + b) given off(s0) and C = s0 % 8 (both b and C
+// compile-time), valid for s0 < kRecRing and b < kRecMirror.
+template <int C>
+__device__ __forceinline__ constexpr int rec_step(int b) {
+    return 32 * b + 16 * ((C + b) >> 3);
+}
+
+// Writes 16-byte half `half` of record t (and its mirror).
+__device__ __forceinline__ int rec_slot(int t) { return t % kRecRing; }
+__device__ __forceinline__ void rec_store(char* ring, int t, int half, uint4 v) {
+    const int s = rec_slot(t);
+    *reinterpret_cast<uint4*>(ring + rec_off(s) + 16 * half) = v;
+    if (s < kRecMirror) *reinterpret_cast<uint4*>(ring + rec_off(s + kRecRing) + 16 * half) = v;
+}
+__device__ __forceinline__ uint4 lds128(const char* p) { return *reinterpret_cast<const uint4*>(p); }
+__device__ __forceinline__ uint2 lds64(const char* p) { return *reinterpret_cast<const uint2*>(p); }
 
 }  // namespace mpgpu

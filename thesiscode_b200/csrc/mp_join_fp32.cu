@@ -63,24 +63,27 @@ __device__ __forceinline__ void flush_row(const Fp32TileParams& P, float v, int6
     }
 }
 
+// One chunk = R consecutive columns.  Per column: R cells per lane, the
+// lane's column minimum, then one warp-wide REDUX; lane b keeps the result of
+// column b so the chunk's column flushes happen once, after the chunk, with no
+// divergent branch between steps (consecutive steps can overlap).
 template <int R, bool FAST>
-__device__ __forceinline__ void chunk_fp32(const Fp32TileParams& P, int64_t jc, const RowRec* rowp,
-                                           const RowRec* colp, RowRec (&win)[R / 2],
-                                           unsigned long long (&nc2)[R / 2], float (&acc)[2 * R - 1],
-                                           const unsigned (&tag)[R], const int64_t (&lim)[R],
-                                           int64_t gb, int lane, float ulim) {
+__device__ __forceinline__ void chunk_fp32(const char* rbase, const char* cbuf,
+                                           RowRec (&win)[R / 2], unsigned long long (&nc2)[R / 2],
+                                           float (&acc)[2 * R - 1], const unsigned (&tag)[R],
+                                           const int (&limr)[R], int jr, int lane, int& colkey) {
     constexpr int H = R / 2;
     const unsigned long long one2 = f2_pack(1.0f, 1.0f);
 #pragma unroll
     for (int b = 0; b < R; ++b) {
-        const int64_t j = jc + b;
         {
-            const RowRec* src = rowp + jc + b + H - 1;
-            win[(b + H - 1) % H].dfdg = __ldg(&src->dfdg);
-            win[(b + H - 1) % H].nn = __ldg(&src->nn);
+            // record tbase + b + H - 1; tbase % 8 == 0, so its slot % 8 == H - 1
+            const char* p = rbase + rec_step<H - 1>(b);
+            win[(b + H - 1) % H].dfdg = *reinterpret_cast<const ulonglong2*>(p);
+            win[(b + H - 1) % H].nn = *reinterpret_cast<const unsigned long long*>(p + 16);
         }
-        const ulonglong2 cdfdg = __ldg(&colp[j].dfdg);
-        const unsigned long long cnn = __ldg(&colp[j].nn);
+        const ulonglong2 cdfdg = *reinterpret_cast<const ulonglong2*>(cbuf + 32 * b);
+        const unsigned long long cnn = *reinterpret_cast<const unsigned long long*>(cbuf + 32 * b + 16);
         float cmin = kInf;
 #pragma unroll
         for (int a = 0; a < H; ++a) {
@@ -94,28 +97,21 @@ __device__ __forceinline__ void chunk_fp32(const Fp32TileParams& P, int64_t jc, 
             float k0 = tag_key(u0, tag[a]);
             float k1 = tag_key(u1, tag[a + H]);
             if (!FAST) {
-                if (j >= lim[a]) k0 = kInf;
-                if (j >= lim[a + H]) k1 = kInf;
+                if (jr + b >= limr[a]) k0 = kInf;
+                if (jr + b >= limr[a + H]) k1 = kInf;
             }
             acc[b + a] = fminf(acc[b + a], k0);
             acc[b + a + H] = fminf(acc[b + a + H], k1);
             cmin = fmin3(cmin, k0, k1);
         }
         const int kmin = __reduce_min_sync(kFullMask, __float_as_int(cmin));
-        if (lane == 0) {
-            const unsigned bits = (unsigned)kmin;
-            const float u = untag_value(bits);
-            if (u < ulim) {
-                const unsigned t = bits & kTagMask;
-                const int64_t q = j + gb + (int64_t)(t >> 3) * R + (t & 7u);
-                atomicMin(P.key + j, ((unsigned long long)ord_f32(u) << 32) | (unsigned long long)q);
-            }
-        }
+        colkey = (lane == b) ? kmin : colkey;
     }
 }
 
 template <int R>
-__device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, int lane, float* ring) {
+__device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, int lane, float* ring,
+                          char* rring, char* cring) {
     constexpr int H = R / 2;
     constexpr int RING = 32 * R;
     const int64_t gb = P.g_lo + band * (int64_t)RING;
@@ -126,14 +122,15 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
     if (j0 >= j1) return;
     const float ulim = (float)(1.0 + 1.0 / (double)P.m);
 
-    int64_t lim[R];
-    int64_t minlim = INT64_MAX;
+    // cell (column j, diagonal g) is evaluated iff j - j0 < limr
+    int limr[R];
+    int minlim = INT32_MAX;
     unsigned tag[R];
 #pragma unroll
     for (int a = 0; a < R; ++a) {
         const int64_t g = g0 + a;
-        lim[a] = (g < P.g_hi) ? min(P.PL - g, j1) : 0;
-        minlim = min(minlim, lim[a]);
+        limr[a] = (g < P.g_hi) ? (int)(min(P.PL - g, j1) - j0) : 0;
+        minlim = min(minlim, limr[a]);
         tag[a] = ((unsigned)lane << 3) | (unsigned)a;
     }
 
@@ -181,21 +178,56 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
 #pragma unroll
     for (int k = 0; k < 2 * R - 1; ++k) acc[k] = kInf;
 
-    const RowRec* rowp = reinterpret_cast<const RowRec*>(P.rowrec) + g0;
-    const RowRec* colp = reinterpret_cast<const RowRec*>(P.colrec);
+    // row records of the band, tile-relative index t = row - (j0 + gb), staged
+    // in the warp's shared-memory ring; before chunk c it holds t < fill
+    const uint4* rsrc = reinterpret_cast<const uint4*>(
+        reinterpret_cast<const RowRec*>(P.rowrec) + (j0 + gb));
+    int fill = 33 * R + H;
+    for (int i = lane; i < 2 * fill; i += 32) rec_store(rring, i >> 1, i & 1, __ldg(rsrc + i));
+    __syncwarp();
+    // column records, double-buffered per chunk (R records of 32 bytes each)
+    const uint4* csrc = reinterpret_cast<const uint4*>(
+        reinterpret_cast<const RowRec*>(P.colrec) + j0);
+    if (lane < 2 * R) *reinterpret_cast<uint4*>(cring + 16 * lane) = __ldg(csrc + lane);
+    __syncwarp();
     RowRec win[H];
 #pragma unroll
     for (int k = 0; k < H - 1; ++k) {
-        win[k].dfdg = __ldg(&rowp[j0 + k].dfdg);
-        win[k].nn = __ldg(&rowp[j0 + k].nn);
+        const char* p = rring + rec_off(rec_slot(lane * R + k));
+        win[k].dfdg = *reinterpret_cast<const ulonglong2*>(p);
+        win[k].nn = *reinterpret_cast<const unsigned long long*>(p + 16);
     }
 
+    int cb = 0;  // column buffer holding the current chunk
     for (int64_t jc = j0; jc < j1; jc += R) {
-        const bool fast = __all_sync(kFullMask, jc + R <= minlim);
+        const int jr = (int)(jc - j0);
+        // prefetch what the next chunk appends: R row records (lanes 0..2R-1)
+        // and R column records (lanes 2R..4R-1), 16 bytes per lane
+        uint4 next = (lane < 2 * R) ? __ldg(rsrc + 2 * fill + lane)
+                                    : __ldg(csrc + 2 * (jr + R) + (lane - 2 * R));
+        const char* rbase = rring + rec_off(rec_slot(jr + lane * R + H - 1));
+        int colkey = 0x7fffffff;
+        const char* cbuf = cring + cb * 32 * R;
+        const bool fast = __all_sync(kFullMask, jr + R <= minlim);
         if (fast)
-            chunk_fp32<R, true>(P, jc, rowp, colp, win, nc2, acc, tag, lim, gb, lane, ulim);
+            chunk_fp32<R, true>(rbase, cbuf, win, nc2, acc, tag, limr, jr, lane, colkey);
         else
-            chunk_fp32<R, false>(P, jc, rowp, colp, win, nc2, acc, tag, lim, gb, lane, ulim);
+            chunk_fp32<R, false>(rbase, cbuf, win, nc2, acc, tag, limr, jr, lane, colkey);
+        // column jc + lane's warp minimum (lanes 0..R-1)
+        if (lane < R) {
+            const unsigned bits = (unsigned)colkey;
+            const float u = untag_value(bits);
+            if (u < ulim) {
+                const unsigned t = bits & kTagMask;
+                const int64_t j = jc + lane;
+                const int64_t q = j + gb + (int64_t)(t >> 3) * R + (t & 7u);
+                atomicMin(P.key + j, ((unsigned long long)ord_f32(u) << 32) | (unsigned long long)q);
+            }
+        }
+        if (lane < 2 * R) rec_store(rring, fill + (lane >> 1), lane & 1, next);
+        else *reinterpret_cast<uint4*>(cring + (cb ^ 1) * 32 * R + 16 * (lane - 2 * R)) = next;
+        cb ^= 1;
+        fill += R;
 
         // lower half: rows jc + g0 + [0, R) are finished for this lane
         const int base = (int)((((jc - j0) / R) + lane) % 32) * R;
@@ -242,11 +274,21 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
 constexpr int kFp32WarpsPerBlock = 4;
 
 template <int R>
-__global__ void __launch_bounds__(32 * kFp32WarpsPerBlock)
+constexpr int fp32_smem_bytes() {
+    return kFp32WarpsPerBlock * (kRecRingBytes + 32 * R * (int)sizeof(float) + 2 * 32 * R);
+}
+
+template <int R>
+__global__ void __launch_bounds__(32 * kFp32WarpsPerBlock, 4)
     fp32_tile_kernel(const Fp32TileParams P, int64_t first_tile, int64_t count) {
-    __shared__ __align__(16) float ring_all[kFp32WarpsPerBlock][32 * R];
+    extern __shared__ __align__(128) char smem_fp32[];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
+    char* rring = smem_fp32 + w * kRecRingBytes;
+    float* ring = reinterpret_cast<float*>(smem_fp32 + kFp32WarpsPerBlock * kRecRingBytes) +
+                  w * 32 * R;
+    char* cring = smem_fp32 + kFp32WarpsPerBlock * (kRecRingBytes + 32 * R * (int)sizeof(float)) +
+                  w * 2 * 32 * R;
     const int64_t t = (int64_t)blockIdx.x * kFp32WarpsPerBlock + w;
     if (t >= count) return;
     // tile t -> band pair p, slot s; the pair's bands k and nbands-1-k have
@@ -259,14 +301,14 @@ __global__ void __launch_bounds__(32 * kFp32WarpsPerBlock)
     const int64_t span = 32 * R;
     const int64_t nseg0 = (P.PL - (P.g_lo + p * span) + P.K - 1) / P.K;
     if (s < nseg0) {
-        tile_fp32<R>(P, p, s, lane, ring_all[w]);
+        tile_fp32<R>(P, p, s, lane, ring, rring, cring);
         return;
     }
     s -= nseg0;
     const int64_t p2 = P.nbands - 1 - p;
     if (p2 <= p) return;
     const int64_t nseg1 = (P.PL - (P.g_lo + p2 * span) + P.K - 1) / P.K;
-    if (s < nseg1) tile_fp32<R>(P, p2, s, lane, ring_all[w]);
+    if (s < nseg1) tile_fp32<R>(P, p2, s, lane, ring, rring, cring);
 }
 
 }  // namespace
@@ -274,8 +316,14 @@ __global__ void __launch_bounds__(32 * kFp32WarpsPerBlock)
 template <int R>
 void launch_fp32_tiles(const Fp32TileParams& P, int64_t first_tile, int64_t count, cudaStream_t s) {
     const int64_t blocks = (count + kFp32WarpsPerBlock - 1) / kFp32WarpsPerBlock;
+    constexpr int smem = fp32_smem_bytes<R>();
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(fp32_tile_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        configured = true;
+    }
     if (blocks > 0)
-        fp32_tile_kernel<R><<<(unsigned)blocks, 32 * kFp32WarpsPerBlock, 0, s>>>(P, first_tile, count);
+        fp32_tile_kernel<R><<<(unsigned)blocks, 32 * kFp32WarpsPerBlock, smem, s>>>(P, first_tile, count);
 }
 
 template void launch_fp32_tiles<8>(const Fp32TileParams&, int64_t, int64_t, cudaStream_t);

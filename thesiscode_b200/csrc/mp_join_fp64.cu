@@ -40,6 +40,16 @@ __device__ __forceinline__ double4 ld_rec(const double4* p) {
     return make_double4(lo.x, lo.y, hi.x, hi.y);
 }
 
+__device__ __forceinline__ double u2d(unsigned lo, unsigned hi) {
+    return __hiloint2double((int)hi, (int)lo);
+}
+// A 32-byte record of the warp's shared-memory ring.
+__device__ __forceinline__ double4 ring_rec(const char* p) {
+    const uint4 a = lds128(p);
+    const uint4 b = lds128(p + 16);
+    return make_double4(u2d(a.x, a.y), u2d(a.z, a.w), u2d(b.x, b.y), u2d(b.z, b.w));
+}
+
 __device__ __forceinline__ void flush_fp64(const Fp64BandParams& P, int shard, int64_t slot,
                                            double score, int64_t neighbour) {
     unsigned long long* ke = P.kexact + (int64_t)shard * P.key_stride + slot;
@@ -48,19 +58,29 @@ __device__ __forceinline__ void flush_fp64(const Fp64BandParams& P, int shard, i
     atomicMax(ki, idx_key_f64(score, P.m, (unsigned long long)neighbour, P.idx_bits));
 }
 
+// One chunk = R consecutive columns.  Per column the lanes' best cells are
+// reduced across the warp with two REDUX instructions (high, then low word of
+// the ordered score); the lowest winning lane parks (score, row) in the
+// warp's column slot with a predicated store, so no divergent branch splits
+// consecutive steps.  The slots are flushed once per chunk.
 template <int R, bool FAST>
-__device__ __forceinline__ void chunk_fp64(const Fp64BandParams& P, int64_t jc, const double4* rowp,
-                                           double4 (&rwin)[R], double (&qt)[R],
-                                           const int64_t (&len)[R], const int64_t (&psw)[R],
+__device__ __forceinline__ void chunk_fp64(const Fp64BandParams& P, int64_t jc, const char* rring,
+                                           const char* rbase, int tbase, double4 (&rwin)[R], double (&qt)[R],
+                                           const int (&len)[R], const int (&psw)[R],
                                            double (&acc_s)[2 * R - 1], int (&acc_a)[2 * R - 1],
-                                           int64_t g0, int lane, int shard) {
+                                           int64_t g0, int lane, double* cslot_s, int* cslot_r) {
 #pragma unroll
     for (int b = 0; b < R; ++b) {
         const int64_t j = jc + b;
-        rwin[(b + R - 1) % R] = ld_rec(rowp + jc + b + R - 1);
+        // record tbase + b + R - 1 (tbase = jc + lane*R): with R = 8 the slot of
+        // record tbase + R - 1 is 7 mod 8 and the step offsets are constants
+        if (R == 8)
+            rwin[(b + R - 1) % R] = ring_rec(rbase + rec_step<7>(b));
+        else
+            rwin[(b + R - 1) % R] =
+                ring_rec(rring + rec_off(rec_slot(tbase + b + R - 1)));
         const double4 cv = ld_rec(P.colrec + j);
-        double cbest = -DBL_MAX;
-        int ca = 0;
+        double sc[R];
 #pragma unroll
         for (int a = 0; a < R; ++a) {
             const double4 rv = rwin[(b + a) % R];
@@ -86,31 +106,46 @@ __device__ __forceinline__ void chunk_fp64(const Fp64BandParams& P, int64_t jc, 
             } else {
                 score = -DBL_MAX;
             }
+            sc[a] = score;
             if (score > acc_s[b + a]) {
                 acc_s[b + a] = score;
                 acc_a[b + a] = a;
             }
-            if (score > cbest) {
-                cbest = score;
-                ca = a;
-            }
         }
-        // column j: warp maximum of the lanes' bests, by ordered key
+        // lane's best cell of column j: pairwise tree, left wins ties
+        double cb[R];
+        int ca[R];
+#pragma unroll
+        for (int a = 0; a < R; ++a) {
+            cb[a] = sc[a];
+            ca[a] = a;
+        }
+#pragma unroll
+        for (int w = 1; w < R; w *= 2)
+#pragma unroll
+            for (int a = 0; a + w < R; a += 2 * w)
+                if (cb[a + w] > cb[a]) {
+                    cb[a] = cb[a + w];
+                    ca[a] = ca[a + w];
+                }
+        const double cbest = cb[0];
         const unsigned long long key = (cbest > P.floor) ? ord_f64(cbest) : 0ull;
         const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
         const unsigned mhi = __reduce_max_sync(kFullMask, hi);
-        if (mhi != 0u) {
-            const unsigned mlo = __reduce_max_sync(kFullMask, hi == mhi ? lo : 0u);
-            const unsigned win = __ballot_sync(kFullMask, hi == mhi && lo == mlo);
-            if (lane == __ffs(win) - 1)
-                flush_fp64(P, shard, j + P.col_key_off, cbest, j + g0 + ca + P.row_nb_off);
+        const unsigned mlo = __reduce_max_sync(kFullMask, hi == mhi ? lo : 0u);
+        const bool top = (hi == mhi) && (lo == mlo) && (mhi != 0u);
+        const unsigned tops = __ballot_sync(kFullMask, top);
+        if (top && (tops & ((1u << lane) - 1u)) == 0u) {
+            cslot_s[b] = cbest;
+            cslot_r[b] = (int)(j + g0 + ca[0] - jc);  // row - jc, small and non-negative
         }
     }
 }
 
 template <int R>
 __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band, int lane,
-                                          int shard, double* ring_s, int* ring_c) {
+                                          int shard, double* ring_s, int* ring_c, char* rring,
+                                          double* cslot_s, int* cslot_r) {
     constexpr int RING = 32 * R;
     const int64_t gb = P.g_lo + band * (int64_t)RING;
     const int64_t g0 = gb + (int64_t)lane * R;
@@ -118,8 +153,8 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
     if (jmax <= 0) return;
 
     double qt[R];
-    int64_t len[R], psw[R];
-    int64_t minpsw = INT64_MAX;
+    int len[R], psw[R];  // columns < 2^31 (checked by the host)
+    int minpsw = INT32_MAX;
 #pragma unroll
     for (int a = 0; a < R; ++a) {
         const int64_t g = g0 + a;
@@ -127,8 +162,8 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
             const int64_t delta = (g - P.blk_origin) % P.B;
             const int64_t T = P.Tbase - (g - delta);
             qt[a] = P.qt0[g - P.g_lo];
-            len[a] = T - delta;
-            psw[a] = (delta < (P.B & ~3ll)) ? T - 4 * (delta / 4 + 1) : -1;
+            len[a] = (int)(T - delta);
+            psw[a] = (delta < (P.B & ~3ll)) ? (int)(T - 4 * (delta / 4 + 1)) : -1;
         } else {
             qt[a] = 0.0;
             len[a] = 0;
@@ -137,11 +172,12 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
         minpsw = min(minpsw, psw[a]);
     }
 
-    // ring of row partials, slot = (r - gb) mod RING
+    // ring of row partials, slot = (r - gb) mod RING; column slots of a chunk
     for (int k = lane; k < RING; k += 32) {
         ring_s[k] = -DBL_MAX;
         ring_c[k] = 0;
     }
+    if (lane < R) cslot_s[lane] = -DBL_MAX;
     __syncwarp();
 
     double acc_s[2 * R - 1];
@@ -152,18 +188,40 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
         acc_a[k] = 0;
     }
 
+    // row records of the band (t = row - gb) staged in the warp's shared-memory
+    // ring; before chunk jc it holds t < fill
+    const uint4* rsrc = reinterpret_cast<const uint4*>(P.rowrec + gb);
+    int fill = 34 * R;
+    for (int i = lane; i < 2 * fill; i += 32) rec_store(rring, i >> 1, i & 1, __ldg(rsrc + i));
+    __syncwarp();
     // register window of row records: slot (k mod R) holds row g0 + jc + k
     double4 rwin[R];
-    const double4* rowp = P.rowrec + g0;
 #pragma unroll
-    for (int k = 0; k < R - 1; ++k) rwin[k] = ld_rec(rowp + k);
+    for (int k = 0; k < R - 1; ++k) rwin[k] = ring_rec(rring + rec_off(rec_slot(lane * R + k)));
 
     for (int64_t jc = 0; jc < jmax; jc += R) {
+        uint4 next = make_uint4(0, 0, 0, 0);
+        if (lane < 2 * R) next = __ldg(rsrc + 2 * fill + lane);
+        const int tbase = (int)jc + lane * R;
+        const char* rbase = rring + rec_off(rec_slot(tbase + R - 1));
         const bool fast = __all_sync(kFullMask, jc + R - 1 <= minpsw);
         if (fast)
-            chunk_fp64<R, true>(P, jc, rowp, rwin, qt, len, psw, acc_s, acc_a, g0, lane, shard);
+            chunk_fp64<R, true>(P, jc, rring, rbase, tbase, rwin, qt, len, psw, acc_s, acc_a, g0, lane,
+                                cslot_s, cslot_r);
         else
-            chunk_fp64<R, false>(P, jc, rowp, rwin, qt, len, psw, acc_s, acc_a, g0, lane, shard);
+            chunk_fp64<R, false>(P, jc, rring, rbase, tbase, rwin, qt, len, psw, acc_s, acc_a, g0, lane,
+                                 cslot_s, cslot_r);
+        __syncwarp();
+        // the chunk's column maxima (one per column, parked by the winning lane)
+        if (lane < R) {
+            const double cs = cslot_s[lane];
+            if (cs > P.floor)
+                flush_fp64(P, shard, jc + lane + P.col_key_off, cs,
+                           jc + cslot_r[lane] + P.row_nb_off);
+            cslot_s[lane] = -DBL_MAX;
+        }
+        if (lane < 2 * R) rec_store(rring, fill + (lane >> 1), lane & 1, next);
+        fill += R;
         // rows jc + g0 + [0, R) are done for this lane: merge into the ring
         const int base = (int)(((jc / R) + lane) % 32) * R;
 #pragma unroll
@@ -220,18 +278,34 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
 }
 
 template <int R>
+constexpr int fp64_smem_bytes() {
+    return kFp64WarpsPerBlock *
+           (kRecRingBytes + (32 * R + R) * (int)(sizeof(double) + sizeof(int)));
+}
+
+template <int R>
 __global__ void __launch_bounds__(32 * kFp64WarpsPerBlock) fp64_band_kernel(const Fp64BandParams P) {
-    __shared__ double ring_s_all[kFp64WarpsPerBlock][32 * R];
-    __shared__ int ring_c_all[kFp64WarpsPerBlock][32 * R];
+    extern __shared__ __align__(128) char smem_fp64[];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
+    char* rring = smem_fp64 + w * kRecRingBytes;
+    double* ring_s = reinterpret_cast<double*>(smem_fp64 + kFp64WarpsPerBlock * kRecRingBytes) +
+                     w * 32 * R;
+    int* ring_c = reinterpret_cast<int*>(smem_fp64 + kFp64WarpsPerBlock * kRecRingBytes +
+                                         kFp64WarpsPerBlock * 32 * R * sizeof(double)) +
+                  w * 32 * R;
+    double* cslot_s = reinterpret_cast<double*>(
+                          smem_fp64 + kFp64WarpsPerBlock * kRecRingBytes +
+                          kFp64WarpsPerBlock * 32 * R * (sizeof(double) + sizeof(int))) +
+                      w * R;
+    int* cslot_r = reinterpret_cast<int*>(cslot_s + (kFp64WarpsPerBlock - w) * R) + w * R;
     const int64_t job = (int64_t)blockIdx.x * kFp64WarpsPerBlock + w;
     const int64_t njobs = (P.nbands + 1) / 2;
     if (job >= njobs) return;
     const int shard = (int)(job % P.shards);
-    band_fp64<R>(P, job, lane, shard, ring_s_all[w], ring_c_all[w]);
+    band_fp64<R>(P, job, lane, shard, ring_s, ring_c, rring, cslot_s, cslot_r);
     const int64_t partner = P.nbands - 1 - job;
-    if (partner > job) band_fp64<R>(P, partner, lane, shard, ring_s_all[w], ring_c_all[w]);
+    if (partner > job) band_fp64<R>(P, partner, lane, shard, ring_s, ring_c, rring, cslot_s, cslot_r);
 }
 
 }  // namespace
@@ -240,7 +314,13 @@ template <int R>
 void launch_fp64_band(const Fp64BandParams& P, cudaStream_t s) {
     const int64_t njobs = (P.nbands + 1) / 2;
     const int64_t blocks = (njobs + kFp64WarpsPerBlock - 1) / kFp64WarpsPerBlock;
-    if (blocks > 0) fp64_band_kernel<R><<<(unsigned)blocks, 32 * kFp64WarpsPerBlock, 0, s>>>(P);
+    constexpr int smem = fp64_smem_bytes<R>();
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(fp64_band_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        configured = true;
+    }
+    if (blocks > 0) fp64_band_kernel<R><<<(unsigned)blocks, 32 * kFp64WarpsPerBlock, smem, s>>>(P);
 }
 
 template void launch_fp64_band<1>(const Fp64BandParams&, cudaStream_t);
