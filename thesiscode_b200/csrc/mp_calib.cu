@@ -13,25 +13,21 @@ namespace mpgpu {
 namespace {
 
 __global__ void peak_f32x2_kernel(float* out, int iters) {
-    unsigned long long a[8];
+    float2 a[8];
     const float s = 1.0f + 1e-7f * (float)threadIdx.x;
-    const unsigned long long mul = f2_pack(0.999999f, 0.999998f);
-    const unsigned long long add = f2_pack(1e-7f, 2e-7f);
+    const float2 mul = make_float2(0.999999f, 0.999998f);
+    const float2 add = make_float2(1e-7f, 2e-7f);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) a[k] = f2_pack(s + k, s - k);
+    for (int k = 0; k < 8; ++k) a[k] = make_float2(s + k, s - k);
     for (int i = 0; i < iters; ++i) {
 #pragma unroll
         for (int u = 0; u < 4; ++u)
 #pragma unroll
-            for (int k = 0; k < 8; ++k) a[k] = f2_fma(a[k], mul, add);
+            for (int k = 0; k < 8; ++k) a[k] = __ffma2_rn(a[k], mul, add);
     }
     float acc = 0.f;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        float x, y;
-        f2_unpack(a[k], x, y);
-        acc += x + y;
-    }
+    for (int k = 0; k < 8; ++k) acc += a[k].x + a[k].y;
     if (acc == 12345.678f) out[threadIdx.x] = acc;
 }
 

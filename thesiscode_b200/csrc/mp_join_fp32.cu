@@ -34,10 +34,13 @@ namespace mpgpu {
 namespace {
 
 struct RowRec {
-    ulonglong2 dfdg;         // (df[j], df[j+H]), (dg[j], dg[j+H])
-    unsigned long long nn;   // (nn[j], nn[j+H])
-    unsigned long long pad;
+    float4 dfdg;  // (df[j], df[j+H], dg[j], dg[j+H])
+    float4 nn1;   // (nn[j], nn[j+H], 1, 1): the constant pair rides along with the
+                  // record so the fused u = 1 + nc*nn never needs a
+                  // rematerialised immediate register pair
 };
+__device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4& v) { return make_float2(v.z, v.w); }
 static_assert(sizeof(RowRec) == 32, "row record is 32 bytes");
 
 constexpr unsigned kTagMask = 0xffu;
@@ -64,48 +67,47 @@ __device__ __forceinline__ void flush_row(const Fp32TileParams& P, float v, int6
 }
 
 // One chunk = R consecutive columns.  Per column: R cells per lane, the
-// lane's column minimum, then one warp-wide REDUX; lane b keeps the result of
-// column b so the chunk's column flushes happen once, after the chunk, with no
-// divergent branch between steps (consecutive steps can overlap).
-template <int R, bool FAST>
+// lane's column minimum, then one warp-wide REDUX; lane OFF + b keeps the
+// result of column b so the column flushes happen once per chunk pair, with
+// no divergent branch between steps (consecutive steps can overlap).  Row
+// partials live in a 2R-entry circular register array; OFF (0 or R) is the
+// chunk's rotation, so no register ever moves between chunks.
+template <int R, bool FAST, int OFF>
 __device__ __forceinline__ void chunk_fp32(const char* rbase, const char* cbuf,
-                                           RowRec (&win)[R / 2], unsigned long long (&nc2)[R / 2],
-                                           float (&acc)[2 * R - 1], const unsigned (&tag)[R],
+                                           RowRec (&win)[R / 2], float2 (&nc2)[R / 2],
+                                           float (&acc)[2 * R], const unsigned (&tag)[R],
                                            const int (&limr)[R], int jr, int lane, int& colkey) {
     constexpr int H = R / 2;
-    const unsigned long long one2 = f2_pack(1.0f, 1.0f);
 #pragma unroll
     for (int b = 0; b < R; ++b) {
         {
             // record tbase + b + H - 1; tbase % 8 == 0, so its slot % 8 == H - 1
             const char* p = rbase + rec_step<H - 1>(b);
-            win[(b + H - 1) % H].dfdg = *reinterpret_cast<const ulonglong2*>(p);
-            win[(b + H - 1) % H].nn = *reinterpret_cast<const unsigned long long*>(p + 16);
+            win[(b + H - 1) % H].dfdg = *reinterpret_cast<const float4*>(p);
+            win[(b + H - 1) % H].nn1 = *reinterpret_cast<const float4*>(p + 16);
         }
-        const ulonglong2 cdfdg = *reinterpret_cast<const ulonglong2*>(cbuf + 32 * b);
-        const unsigned long long cnn = *reinterpret_cast<const unsigned long long*>(cbuf + 32 * b + 16);
+        const float4 cv = *reinterpret_cast<const float4*>(cbuf + 32 * b);
+        const float2 cnn = *reinterpret_cast<const float2*>(cbuf + 32 * b + 16);
         float cmin = kInf;
 #pragma unroll
         for (int a = 0; a < H; ++a) {
             const RowRec& rv = win[(b + a) % H];
-            const unsigned long long nn2 = f2_mul(cnn, rv.nn);
-            const unsigned long long u2 = f2_fma(nc2[a], nn2, one2);
-            nc2[a] = f2_fma(cdfdg.x, rv.dfdg.y, nc2[a]);
-            nc2[a] = f2_fma(rv.dfdg.x, cdfdg.y, nc2[a]);
-            float u0, u1;
-            f2_unpack(u2, u0, u1);
-            float k0 = tag_key(u0, tag[a]);
-            float k1 = tag_key(u1, tag[a + H]);
+            const float2 nn2 = __fmul2_rn(cnn, lo2(rv.nn1));
+            const float2 u2 = __ffma2_rn(nc2[a], nn2, hi2(rv.nn1));
+            nc2[a] = __ffma2_rn(lo2(cv), hi2(rv.dfdg), nc2[a]);
+            nc2[a] = __ffma2_rn(lo2(rv.dfdg), hi2(cv), nc2[a]);
+            float k0 = tag_key(u2.x, tag[a]);
+            float k1 = tag_key(u2.y, tag[a + H]);
             if (!FAST) {
                 if (jr + b >= limr[a]) k0 = kInf;
                 if (jr + b >= limr[a + H]) k1 = kInf;
             }
-            acc[b + a] = fminf(acc[b + a], k0);
-            acc[b + a + H] = fminf(acc[b + a + H], k1);
+            acc[(b + a + OFF) % (2 * R)] = fminf(acc[(b + a + OFF) % (2 * R)], k0);
+            acc[(b + a + H + OFF) % (2 * R)] = fminf(acc[(b + a + H + OFF) % (2 * R)], k1);
             cmin = fmin3(cmin, k0, k1);
         }
         const int kmin = __reduce_min_sync(kFullMask, __float_as_int(cmin));
-        colkey = (lane == b) ? kmin : colkey;
+        colkey = (lane == b + OFF) ? kmin : colkey;
     }
 }
 
@@ -160,135 +162,161 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
             for (int a = 0; a < R; ++a) q[a] = __fma_rn(x, __ldg(Aw + k + a), q[a]);
         }
     }
-    unsigned long long nc2[H];
+    float2 nc2[H];
     {
         const double mu0 = (double)P.m * __ldg(P.mean + j0);
         float nc[R];
 #pragma unroll
         for (int a = 0; a < R; ++a) nc[a] = (float)__fma_rn(mu0, __ldg(P.mean + j0 + g0 + a), -q[a]);
 #pragma unroll
-        for (int a = 0; a < H; ++a) nc2[a] = f2_pack(nc[a], nc[a + H]);
+        for (int a = 0; a < H; ++a) nc2[a] = make_float2(nc[a], nc[a + H]);
     }
 
-    // ---- ring of row partials for this tile: slot = (r - j0 - gb) mod RING --
-    for (int k = lane; k < RING; k += 32) ring[k] = kInf;
+    // ---- ring of row partials for this tile -----------------------------------
+    for (int k = lane; k < 34 * R; k += 32) ring[k] = kInf;
     __syncwarp();
 
-    float acc[2 * R - 1];
+    // row partials: row o of chunk c (o in [0, 2R-1)) lives in acc[(o + R*(c%2)) % 2R]
+    float acc[2 * R];
 #pragma unroll
-    for (int k = 0; k < 2 * R - 1; ++k) acc[k] = kInf;
+    for (int k = 0; k < 2 * R; ++k) acc[k] = kInf;
 
     // row records of the band, tile-relative index t = row - (j0 + gb), staged
-    // in the warp's shared-memory ring; before chunk c it holds t < fill
+    // in the warp's shared-memory ring; before chunk pair i it holds t < fill
     const uint4* rsrc = reinterpret_cast<const uint4*>(
         reinterpret_cast<const RowRec*>(P.rowrec) + (j0 + gb));
     int fill = 33 * R + H;
     for (int i = lane; i < 2 * fill; i += 32) rec_store(rring, i >> 1, i & 1, __ldg(rsrc + i));
-    __syncwarp();
-    // column records, double-buffered per chunk (R records of 32 bytes each)
+    // column records of a chunk pair (2R records), double-buffered
     const uint4* csrc = reinterpret_cast<const uint4*>(
         reinterpret_cast<const RowRec*>(P.colrec) + j0);
-    if (lane < 2 * R) *reinterpret_cast<uint4*>(cring + 16 * lane) = __ldg(csrc + lane);
+    *reinterpret_cast<uint4*>(cring + 16 * lane) = __ldg(csrc + lane);
     __syncwarp();
     RowRec win[H];
 #pragma unroll
     for (int k = 0; k < H - 1; ++k) {
         const char* p = rring + rec_off(rec_slot(lane * R + k));
-        win[k].dfdg = *reinterpret_cast<const ulonglong2*>(p);
-        win[k].nn = *reinterpret_cast<const unsigned long long*>(p + 16);
+        win[k].dfdg = *reinterpret_cast<const float4*>(p);
+        win[k].nn1 = *reinterpret_cast<const float4*>(p + 16);
     }
 
-    int cb = 0;  // column buffer holding the current chunk
-    for (int64_t jc = j0; jc < j1; jc += R) {
-        const int jr = (int)(jc - j0);
-        // prefetch what the next chunk appends: R row records (lanes 0..2R-1)
-        // and R column records (lanes 2R..4R-1), 16 bytes per lane
-        uint4 next = (lane < 2 * R) ? __ldg(rsrc + 2 * fill + lane)
-                                    : __ldg(csrc + 2 * (jr + R) + (lane - 2 * R));
-        const char* rbase = rring + rec_off(rec_slot(jr + lane * R + H - 1));
+    // Row partials leave the registers through a ring of RK slots in shared
+    // memory: row t of the tile sits at ((t / R) % RK_CHUNKS) * R + t % R.
+    // With RK_CHUNKS = 34 the rows finished by lane 0 in a chunk pair stay put
+    // until they are flushed at the end of the pair.
+    constexpr int RK_CHUNKS = 34;
+    int cb = 0;                              // column buffer of the current pair
+    int rslot = rec_slot(lane * R + H - 1);  // record slot of jr + lane*R + H - 1
+    int kslot = lane;                        // (jr / R + lane) % RK_CHUNKS
+    const int ncols = (int)(j1 - j0);
+    int jr = 0;
+    for (; jr < ncols; jr += 2 * R) {
+        // prefetch what the next pair appends: 2R row records and 2R column records
+        const uint4 nrow = __ldg(rsrc + 2 * fill + lane);
+        const uint4 ncol = __ldg(csrc + 2 * (jr + 2 * R) + lane);
         int colkey = 0x7fffffff;
-        const char* cbuf = cring + cb * 32 * R;
-        const bool fast = __all_sync(kFullMask, jr + R <= minlim);
-        if (fast)
-            chunk_fp32<R, true>(rbase, cbuf, win, nc2, acc, tag, limr, jr, lane, colkey);
-        else
-            chunk_fp32<R, false>(rbase, cbuf, win, nc2, acc, tag, limr, jr, lane, colkey);
-        // column jc + lane's warp minimum (lanes 0..R-1)
-        if (lane < R) {
+        const char* cbuf = cring + cb * 64 * R;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int jh = jr + half * R;
+            const char* rbase = rring + rec_off(rslot);
+            rslot += R;
+            if (rslot >= kRecRing) rslot -= kRecRing;
+            const bool fast = __all_sync(kFullMask, jh + R <= minlim);
+            if (half == 0) {
+                if (fast)
+                    chunk_fp32<R, true, 0>(rbase, cbuf, win, nc2, acc, tag, limr, jh, lane, colkey);
+                else
+                    chunk_fp32<R, false, 0>(rbase, cbuf, win, nc2, acc, tag, limr, jh, lane, colkey);
+            } else {
+                if (fast)
+                    chunk_fp32<R, true, R>(rbase, cbuf + 32 * R, win, nc2, acc, tag, limr, jh, lane,
+                                           colkey);
+                else
+                    chunk_fp32<R, false, R>(rbase, cbuf + 32 * R, win, nc2, acc, tag, limr, jh,
+                                            lane, colkey);
+            }
+            // this chunk's lower half (rows jh + g0 + [0, R)) is final for the lane
+            const int ks = (kslot + half) >= RK_CHUNKS ? kslot + half - RK_CHUNKS : kslot + half;
+            float4* rv4 = reinterpret_cast<float4*>(ring + ks * R);
+#pragma unroll
+            for (int v = 0; v < R / 4; ++v) {
+                float4 t = rv4[v];
+                t.x = fminf(t.x, acc[(4 * v + 0 + half * R) % (2 * R)]);
+                t.y = fminf(t.y, acc[(4 * v + 1 + half * R) % (2 * R)]);
+                t.z = fminf(t.z, acc[(4 * v + 2 + half * R) % (2 * R)]);
+                t.w = fminf(t.w, acc[(4 * v + 3 + half * R) % (2 * R)]);
+                rv4[v] = t;
+            }
+#pragma unroll
+            for (int k = 0; k < R; ++k) acc[(k + half * R) % (2 * R)] = kInf;
+        }
+        kslot += 2;
+        if (kslot >= RK_CHUNKS) kslot -= RK_CHUNKS;
+        __syncwarp();
+        // columns jr + [0, 2R): one per lane
+        if (lane < 2 * R) {
             const unsigned bits = (unsigned)colkey;
             const float u = untag_value(bits);
             if (u < ulim) {
                 const unsigned t = bits & kTagMask;
-                const int64_t j = jc + lane;
+                const int64_t j = j0 + jr + lane;
                 const int64_t q = j + gb + (int64_t)(t >> 3) * R + (t & 7u);
                 atomicMin(P.key + j, ((unsigned long long)ord_f32(u) << 32) | (unsigned long long)q);
             }
-        }
-        if (lane < 2 * R) rec_store(rring, fill + (lane >> 1), lane & 1, next);
-        else *reinterpret_cast<uint4*>(cring + (cb ^ 1) * 32 * R + 16 * (lane - 2 * R)) = next;
-        cb ^= 1;
-        fill += R;
-
-        // lower half: rows jc + g0 + [0, R) are finished for this lane
-        const int base = (int)((((jc - j0) / R) + lane) % 32) * R;
-        float4* rv4 = reinterpret_cast<float4*>(ring + base);
-#pragma unroll
-        for (int v = 0; v < R / 4; ++v) {
-            float4 t = rv4[v];
-            t.x = fminf(t.x, acc[4 * v + 0]);
-            t.y = fminf(t.y, acc[4 * v + 1]);
-            t.z = fminf(t.z, acc[4 * v + 2]);
-            t.w = fminf(t.w, acc[4 * v + 3]);
-            rv4[v] = t;
-        }
-        __syncwarp();
-        // rows jc + gb + [0, R) have met every lane of the warp
-        if (lane < R) {
-            const int e = (int)(((jc - j0) / R) % 32) * R + lane;
+            // rows jr + [0, 2R) of the tile have met every lane: flush, free
+            const int c = jr / R + (lane >> 3);
+            const int e = (c % RK_CHUNKS) * R + (lane & (R - 1));
             const float v = ring[e];
             ring[e] = kInf;
-            flush_row<R>(P, v, jc + gb + lane, gb, ulim);
+            flush_row<R>(P, v, j0 + gb + jr + lane, gb, ulim);
         }
+        rec_store(rring, fill + (lane >> 1), lane & 1, nrow);
+        *reinterpret_cast<uint4*>(cring + (cb ^ 1) * 64 * R + 16 * lane) = ncol;
+        cb ^= 1;
+        fill += 2 * R;
         __syncwarp();
-#pragma unroll
-        for (int k = 0; k < R - 1; ++k) acc[k] = acc[k + R];
-#pragma unroll
-        for (int k = R - 1; k < 2 * R - 1; ++k) acc[k] = kInf;
     }
 
-    // drain the rows still in flight
-    const int64_t jend = j0 + ((j1 - j0 + R - 1) / R) * R;
+    // drain: the carried upper half (rows jr + lane*R + [0, R-1)), then every slot
     {
-        const int base = (int)((((jend - j0) / R) + lane) % 32) * R;
+        float* base = ring + kslot * R;
 #pragma unroll
-        for (int k = 0; k < R - 1; ++k) ring[base + k] = fminf(ring[base + k], acc[k]);
+        for (int k = 0; k < R - 1; ++k) base[k] = fminf(base[k], acc[k]);
     }
     __syncwarp();
-    for (int e = lane; e < RING; e += 32) {
-        const int64_t rel = ((int64_t)e - (jend - j0) % RING + RING) % RING;
-        flush_row<R>(P, ring[e], jend + gb + rel, gb, ulim);
+    const int cend = jr / R;
+    for (int e = lane; e < RK_CHUNKS * R; e += 32) {
+        const int cs = e / R;
+        const int rel = (cs - cend % RK_CHUNKS + RK_CHUNKS) % RK_CHUNKS;
+        flush_row<R>(P, ring[e], j0 + gb + (int64_t)(cend + rel) * R + (e % R), gb, ulim);
     }
     __syncwarp();
 }
 
 constexpr int kFp32WarpsPerBlock = 4;
 
+constexpr int kRowKeySlots = 34 * 8;
 template <int R>
 constexpr int fp32_smem_bytes() {
-    return kFp32WarpsPerBlock * (kRecRingBytes + 32 * R * (int)sizeof(float) + 2 * 32 * R);
+    return kFp32WarpsPerBlock * (kRecRingBytes + kRowKeySlots * (int)sizeof(float) + 4 * 32 * R);
 }
 
+#ifndef MPGPU_FP32_MIN_BLOCKS
+#define MPGPU_FP32_MIN_BLOCKS 3  // 3 x 4 warps per SM (measured best of 2, 3, 4)
+#endif
+
 template <int R>
-__global__ void __launch_bounds__(32 * kFp32WarpsPerBlock, 4)
+__global__ void __launch_bounds__(32 * kFp32WarpsPerBlock, MPGPU_FP32_MIN_BLOCKS)
     fp32_tile_kernel(const Fp32TileParams P, int64_t first_tile, int64_t count) {
     extern __shared__ __align__(128) char smem_fp32[];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     char* rring = smem_fp32 + w * kRecRingBytes;
     float* ring = reinterpret_cast<float*>(smem_fp32 + kFp32WarpsPerBlock * kRecRingBytes) +
-                  w * 32 * R;
-    char* cring = smem_fp32 + kFp32WarpsPerBlock * (kRecRingBytes + 32 * R * (int)sizeof(float)) +
-                  w * 2 * 32 * R;
+                  w * kRowKeySlots;
+    char* cring = smem_fp32 + kFp32WarpsPerBlock * (kRecRingBytes + kRowKeySlots * (int)sizeof(float)) +
+                  w * 4 * 32 * R;
     const int64_t t = (int64_t)blockIdx.x * kFp32WarpsPerBlock + w;
     if (t >= count) return;
     // tile t -> band pair p, slot s; the pair's bands k and nbands-1-k have

@@ -190,7 +190,7 @@ __global__ void welford_kernel(const double* __restrict__ A, int64_t m, int64_t 
 //   df[i] = (A[i+m] - A[i]) / 2,  dg[i] = (A[i+m] - mean[i+1]) + (A[i] - mean[i])
 // (zero for the last window, whose successor does not exist), nn[i] = norm[i].
 // Row records are stored as pairs (x[j], x[j+H]) for the f32x2 datapath:
-//   rowrec[j] = {df[j], df[j+H], dg[j], dg[j+H], nn[j], nn[j+H], 0, 0}
+//   rowrec[j] = {df[j], df[j+H], dg[j], dg[j+H], nn[j], nn[j+H], 1, 1}
 // Column records duplicate and negate the column terms:
 //   colrec[p] = {-df[p], -df[p], -dg[p], -dg[p], nn[p], nn[p], 0, 0}
 // Entries past PL read as df = dg = 0, nn = NaN.
@@ -224,7 +224,7 @@ __global__ void pack_fp32_kernel(const double* __restrict__ A, int64_t m, int64_
         fp32_terms(A, m, PL, mean, norm, j, df0, dg0, nn0);
         fp32_terms(A, m, PL, mean, norm, j + H, df1, dg1, nn1);
         rowrec[2 * j] = make_float4(df0, df1, dg0, dg1);
-        rowrec[2 * j + 1] = make_float4(nn0, nn1, 0.f, 0.f);
+        rowrec[2 * j + 1] = make_float4(nn0, nn1, 1.f, 1.f);
         colrec[2 * j] = make_float4(-df0, -df0, -dg0, -dg0);
         colrec[2 * j + 1] = make_float4(nn0, nn0, 0.f, 0.f);
     }
