@@ -46,19 +46,6 @@ def host_cores() -> int:
         return os.cpu_count() or 1
 
 
-def diag_partitions(lo: int, hi: int, parts: int):
-    """Near-equal split of [lo, hi) into `parts` ranges (partitioning_1d.cpp:8-31)."""
-    n = hi - lo
-    full = n - (n // parts) * parts
-    size = n // parts + 1
-    out = []
-    for p in range(parts):
-        first = p * size - max(p - full, 0)
-        last = first + (size if p < full else size - 1)
-        out.append((lo + first, lo + last))
-    return out
-
-
 def sample_range(n: int, m: int, target_cells: float):
     """Diagonal range [excl+1, hi) holding about target_cells cells."""
     PL, lo = n - m + 1, m // 4 + 1
@@ -205,11 +192,9 @@ def run_ours(args, world):
     else:
         x, m = wl.c2()
     n = x.size
+    from thesiscode_b200 import shard
     PL, excl = n - m + 1, m // 4
-    lo_all, hi_all = excl + 1, PL
-    parts = diag_partitions(lo_all, hi_all, 2 * world)
-    mine = [parts[rank], parts[2 * world - 1 - rank]] if world > 1 else [(lo_all, hi_all)]
-    mine = [(a, b) for a, b in mine if b > a]
+    mine = shard.rank_ranges(n, m, rank, world)
     cells_mine = sum(mp.cells(n, m, a, b) for a, b in mine)
     cells_total = mp.cells(n, m)
 
@@ -235,9 +220,9 @@ def run_ours(args, world):
             join_ms += ctx.last_phase_ms()[1]
             if not first:
                 with torch.cuda.stream(stream):
-                    better = (d2b < d2) | ((d2b == d2) & (ixb < ix))
-                    d2.copy_(torch.where(better, d2b, d2))
-                    ix.copy_(torch.where(better, ixb, ix))
+                    md, mi = shard.merge_profiles([d2, d2b], [ix, ixb])
+                    d2.copy_(md)
+                    ix.copy_(mi)
             first = False
         if world > 1:
             with torch.cuda.stream(stream):
@@ -245,12 +230,9 @@ def run_ours(args, world):
                 gi = [torch.empty_like(ix) for _ in range(world)]
                 dist.all_gather(gd, d2)
                 dist.all_gather(gi, ix)
-                D = torch.stack(gd)
-                I = torch.stack(gi)
-                key_best = D.min(dim=0).values
-                cand = torch.where(D == key_best, I, torch.iinfo(torch.int64).max)
-                d2.copy_(key_best)
-                ix.copy_(cand.min(dim=0).values)
+                md, mi = shard.merge_profiles(gd, gi)
+                d2.copy_(md)
+                ix.copy_(mi)
         return launches, join_ms
 
     def timed(precision, steps, warmup):

@@ -1,0 +1,90 @@
+"""Diagonal sharding across ranks (the multi-GPU path) on CPU: world-size-2
+gloo process groups, per-rank partial profiles from the oracle, one
+all-gather merge; the merged profile must equal the single-process join."""
+from __future__ import annotations
+
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as tmp
+
+from thesiscode_b200 import shard, workloads
+
+
+def test_partitions_cover_each_diagonal_once():
+    for n, m, world in [(5000, 64, 2), (5000, 64, 3), (70000, 400, 8), (100, 8, 4)]:
+        PL, excl = n - m + 1, m // 4
+        seen = []
+        for r in range(world):
+            for a, b in shard.rank_ranges(n, m, r, world):
+                seen.extend(range(a, b))
+        assert sorted(seen) == list(range(excl + 1, PL))
+
+
+def test_partition_balance_rule():
+    # rank r takes partitions r and 2P-1-r: cell counts nearly equal per rank
+    n, m, world = 200_000, 256, 4
+    PL = n - m + 1
+    loads = [sum(sum(PL - d for d in range(a, b)) for a, b in shard.rank_ranges(n, m, r, world))
+             for r in range(world)]
+    assert max(loads) / min(loads) < 1.01
+
+
+def test_merge_prefers_smaller_distance_then_index():
+    d2a = np.array([1.0, 2.0, 3.0, 5.0])
+    ia = np.array([7, 8, 9, 4])
+    d2b = np.array([1.0, 1.5, 4.0, 5.0])
+    ib = np.array([3, 2, 1, 6])
+    d2, ix = shard.merge_profiles([d2a, d2b], [ia, ib])
+    assert d2.tolist() == [1.0, 1.5, 3.0, 5.0]
+    assert ix.tolist() == [3, 2, 9, 4]
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, n, m, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle.oracle import Oracle
+        x = workloads.random_walk(n, 5)
+        orc = Oracle()
+
+        def compute(lo, hi):
+            d2, ix = orc.selfjoin(x, m, diag_lo=lo, diag_hi=hi, nthreads=1)
+            return torch.from_numpy(d2), torch.from_numpy(ix)
+
+        d2, ix = shard.distributed_selfjoin(compute, n, m)
+        q.put((rank, d2.numpy(), ix.numpy()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2])
+def test_gloo_sharded_join_equals_single_join(oracle, world):
+    n, m = 4000, 64
+    ctx = tmp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, n, m, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    ref_d2, ref_ix = oracle.selfjoin(workloads.random_walk(n, 5), m)
+    for rank, d2, ix in res:
+        assert np.array_equal(d2, ref_d2), rank
+        assert np.array_equal(ix, ref_ix), rank

@@ -1,0 +1,83 @@
+"""Multi-GPU sharding of one self-join by diagonal ranges.
+
+The reference splits the diagonals of the distance matrix into 2P near-equal
+partitions and gives rank r partitions r and 2P-1-r, so every rank gets one
+long and one short range (scrimppp/src/ScrimpTrivialPar.cpp:200-224, with
+partitioning_1d.cpp:8-31).  Each rank computes a partial profile over its
+ranges; one exchange step -- the reference's MPI_Allreduce with its
+min-by-distance operator (ScrimpTrivialPar.cpp:68-108, 346-357) -- merges them.
+Here the exchange is an all-gather over torch.distributed (NCCL between GPUs,
+gloo in CPU tests) followed by an element-wise arg-min; ties go to the smaller
+neighbour index so the result does not depend on rank order.
+"""
+from __future__ import annotations
+
+from typing import Callable, Sequence
+
+
+def near_equal_split(lo: int, hi: int, parts: int) -> list[tuple[int, int]]:
+    """[lo, hi) cut into `parts` ranges whose sizes differ by at most one,
+    larger ones first (partitioning_1d.cpp:8-31)."""
+    n = hi - lo
+    full = n - (n // parts) * parts
+    size = n // parts + 1
+    out = []
+    for p in range(parts):
+        first = p * size - max(p - full, 0)
+        last = first + (size if p < full else size - 1)
+        out.append((lo + first, lo + last))
+    return out
+
+
+def rank_ranges(n: int, m: int, rank: int, world: int, excl: int = -1) -> list[tuple[int, int]]:
+    """Diagonal ranges [lo, hi) rank `rank` of `world` evaluates."""
+    PL = n - m + 1
+    excl = m // 4 if excl < 0 else excl
+    lo, hi = excl + 1, PL
+    if world == 1:
+        return [(lo, hi)] if hi > lo else []
+    parts = near_equal_split(lo, hi, 2 * world)
+    mine = [parts[rank], parts[2 * world - 1 - rank]]
+    return [(a, b) for a, b in mine if b > a]
+
+
+def merge_profiles(d2s: Sequence, idxs: Sequence):
+    """Element-wise arg-min over partial profiles (numpy or torch arrays):
+    smaller squared distance wins, ties go to the smaller index."""
+    d2, ix = d2s[0], idxs[0]
+    for d, i in zip(d2s[1:], idxs[1:]):
+        better = (d < d2) | ((d == d2) & (i < ix))
+        if hasattr(better, "numpy"):  # torch
+            import torch
+            d2 = torch.where(better, d, d2)
+            ix = torch.where(better, i, ix)
+        else:
+            import numpy as np
+            d2 = np.where(better, d, d2)
+            ix = np.where(better, i, ix)
+    return d2, ix
+
+
+def distributed_selfjoin(compute: Callable, n: int, m: int, group=None):
+    """Runs this rank's diagonal ranges through `compute(diag_lo, diag_hi) ->
+    (d2, idx)` (torch tensors of length PL on this rank's device), merges them
+    locally, then across ranks with one all-gather.  Every rank returns the
+    full profile."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group) if dist.is_initialized() else 1
+    rank = dist.get_rank(group) if dist.is_initialized() else 0
+    ranges = rank_ranges(n, m, rank, world)
+    parts = [compute(a, b) for a, b in ranges]
+    if not parts:
+        PL = n - m + 1
+        parts = [(torch.full((PL,), 2.0 * m + 2.0, dtype=torch.float64),
+                  torch.zeros(PL, dtype=torch.int64))]
+    d2, ix = merge_profiles([p[0] for p in parts], [p[1] for p in parts])
+    if world == 1:
+        return d2, ix
+    gd = [torch.empty_like(d2) for _ in range(world)]
+    gi = [torch.empty_like(ix) for _ in range(world)]
+    dist.all_gather(gd, d2.contiguous(), group=group)
+    dist.all_gather(gi, ix.contiguous(), group=group)
+    return merge_profiles(gd, gi)
