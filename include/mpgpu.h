@@ -124,6 +124,32 @@ int mp_set_phase_timing(mp_context* ctx, int on);
 int mp_last_phase_ms(const mp_context* ctx, double* prep_ms, double* join_ms,
                      double* finalize_ms);
 
+/*
+ * Batched self-joins (no counterpart in the reference: its variants join one
+ * series per process).  A plan fixes `count` series (lengths, windows, FP32
+ * re-anchor interval per series -- NULL = 1024 each -- and input type 0 = double,
+ * 1 = float); all of them are solved by one persistent FP32 re-anchored join
+ * launch, with the preparation and finalisation batched into single launches,
+ * recorded once as a CUDA graph and replayed by every mp_batch_launch.
+ * Results follow mp_selfjoin's conventions.  count <= 65535.
+ *   mp_batch_upload    copies the caller's host series into the plan (pinned staging)
+ *   mp_batch_launch    runs the captured graph on stream (asynchronous)
+ *   mp_batch_download  copies the profiles to the caller's host arrays (synchronous)
+ *   mp_batch_run       the three in order
+ */
+typedef struct mp_batch mp_batch;
+int mp_batch_create(mp_context* ctx, int64_t count, const int64_t* lengths, const int64_t* windows,
+                    const int64_t* reanchor_k, int input_type, mp_batch** out);
+int mp_batch_destroy(mp_batch* b);
+double mp_batch_cells(const mp_batch* b);
+int64_t mp_batch_tiles(const mp_batch* b);
+int64_t mp_batch_launch_count(const mp_batch* b);
+int mp_batch_upload(mp_batch* b, const void* const* series, void* stream);
+int mp_batch_launch(mp_batch* b, void* stream);
+int mp_batch_download(mp_batch* b, double* const* dist2_out, int64_t* const* idx_out, void* stream);
+int mp_batch_run(mp_batch* b, const void* const* series, double* const* dist2_out,
+                 int64_t* const* idx_out, void* stream);
+
 /* FMA throughput of this device's CUDA-core pipes in FLOP/s (2 per FMA),
  * measured with independent FMA chains: which = 0 FP32 (FFMA), 1 FP32 (f32x2
  * FFMA2), 2 FP64 (DFMA).  The join kernels' compute roofline uses it. */

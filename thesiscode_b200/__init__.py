@@ -45,6 +45,9 @@ EXPORTED_SYMBOLS = (
     "mp_selfjoin_scratch_bytes", "mp_selfjoin", "mp_eval_diag_block_triangle",
     "mp_window_stats", "mp_first_qt", "mp_last_launch_count", "mp_list_algorithms",
     "mp_run_algorithm", "mp_set_phase_timing", "mp_last_phase_ms", "mp_measure_fma_peak",
+    "mp_batch_create", "mp_batch_destroy", "mp_batch_cells", "mp_batch_tiles",
+    "mp_batch_launch_count", "mp_batch_upload", "mp_batch_launch", "mp_batch_download",
+    "mp_batch_run",
 )
 
 
@@ -89,6 +92,18 @@ def load_library() -> ctypes.CDLL:
                                    ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(ctypes.c_double)]
     L.mp_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.mp_batch_create.argtypes = [_P, _i64, _P, _P, _P, ctypes.c_int, ctypes.POINTER(_P)]
+    L.mp_batch_destroy.argtypes = [_P]
+    L.mp_batch_cells.argtypes = [_P]
+    L.mp_batch_cells.restype = ctypes.c_double
+    L.mp_batch_tiles.argtypes = [_P]
+    L.mp_batch_tiles.restype = _i64
+    L.mp_batch_launch_count.argtypes = [_P]
+    L.mp_batch_launch_count.restype = _i64
+    L.mp_batch_upload.argtypes = [_P, _P, _P]
+    L.mp_batch_launch.argtypes = [_P, _P]
+    L.mp_batch_download.argtypes = [_P, _P, _P, _P]
+    L.mp_batch_run.argtypes = [_P, _P, _P, _P, _P]
     L.mp_list_algorithms.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     L.mp_run_algorithm.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -240,6 +255,87 @@ class Context:
             self._h, _ptr(prof_colmin), _ptr(idx_colmin), _ptr(prof_rowmin), _ptr(idx_rowmin),
             _ptr(tmpQ), blocklen, trianglen, _ptr(A_hor), _ptr(A_vert), m, _ptr(s_hor),
             _ptr(mu_hor), _ptr(s_vert), _ptr(mu_vert), baserow, basecol, None))
+
+
+class Batch:
+    """Many self-joins in one persistent, graph-captured launch (FP32 form).
+
+    ``lengths``/``windows`` fix the plan; ``reanchor_k`` is one interval per
+    series (None: the autotuned table, see thesiscode_b200.autotune).  Input
+    series are float32 (``input_f32=True``) or float64 numpy arrays."""
+
+    def __init__(self, ctx: Context, lengths, windows, reanchor_k=None, input_f32: bool = True):
+        self._L = ctx._L
+        self._ctx = ctx
+        self.lengths = np.ascontiguousarray(lengths, dtype=np.int64)
+        self.windows = np.ascontiguousarray(windows, dtype=np.int64)
+        if reanchor_k is None:
+            from thesiscode_b200 import autotune
+            reanchor_k = [autotune.lookup(int(n), int(m)) for n, m in zip(self.lengths,
+                                                                          self.windows)]
+        self.reanchor_k = np.ascontiguousarray(reanchor_k, dtype=np.int64)
+        self.input_f32 = input_f32
+        h = _P()
+        rc = self._L.mp_batch_create(ctx._h, self.lengths.size, self.lengths.ctypes.data,
+                                     self.windows.ctypes.data, self.reanchor_k.ctypes.data,
+                                     1 if input_f32 else 0, ctypes.byref(h))
+        if rc != MP_OK:
+            raise MpError(rc, status_string(rc))
+        self._h = h
+        self._keep = []
+
+    @property
+    def cells(self) -> float:
+        return float(self._L.mp_batch_cells(self._h))
+
+    @property
+    def tiles(self) -> int:
+        return int(self._L.mp_batch_tiles(self._h))
+
+    @property
+    def launch_count(self) -> int:
+        return int(self._L.mp_batch_launch_count(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.mp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != MP_OK:
+            raise MpError(rc, status_string(rc))
+
+    def upload(self, series, stream=None):
+        dt = np.float32 if self.input_f32 else np.float64
+        arrs = [np.ascontiguousarray(x, dtype=dt) for x in series]
+        if len(arrs) != self.lengths.size or any(a.size != n for a, n in zip(arrs, self.lengths)):
+            raise ValueError("series do not match the plan")
+        ptrs = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+        self._check(self._L.mp_batch_upload(self._h, ptrs, stream))
+        self._keep = arrs
+
+    def launch(self, stream=None):
+        self._check(self._L.mp_batch_launch(self._h, stream))
+
+    def download(self, stream=None) -> list[Profile]:
+        pls = self.lengths - self.windows + 1
+        d2 = [np.empty(int(p)) for p in pls]
+        ix = [np.empty(int(p), dtype=np.int64) for p in pls]
+        dp = (ctypes.c_void_p * len(d2))(*[a.ctypes.data for a in d2])
+        ip = (ctypes.c_void_p * len(ix))(*[a.ctypes.data for a in ix])
+        self._check(self._L.mp_batch_download(self._h, dp, ip, stream))
+        return [Profile(a, b) for a, b in zip(d2, ix)]
+
+    def run(self, series, stream=None) -> list[Profile]:
+        self.upload(series, stream)
+        self.launch(stream)
+        return self.download(stream)
 
 
 def cells(n: int, m: int, diag_lo: int = 0, diag_hi: int = 0, excl: int = -1) -> int:

@@ -31,6 +31,10 @@ struct mp_context {
     double phase_ms[3] = {-1.0, -1.0, -1.0};
 };
 
+namespace mpgpu {
+size_t ctx_budget(const mp_context* ctx) { return ctx ? ctx->budget : 0; }
+}  // namespace mpgpu
+
 namespace {
 
 constexpr int kThreads = 256;
@@ -208,6 +212,7 @@ size_t fp32_scratch(int64_t n, int64_t m, bool host_io) {
     b += 2 * align_up(8 * (size_t)(PL + kFp32Pad));  // mean, norm
     b += 2 * align_up(32 * (size_t)(PL + kFp32Pad)); // row/col records
     b += align_up(8 * (size_t)PL);               // keys
+    b += align_up(sizeof(Fp32TileParams)) + 256; // descriptor, tile counter
     if (host_io) b += align_up(8 * (size_t)PL) * 2;
     return b + 4096;
 }
@@ -408,6 +413,8 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
     float4* rowrec = cv.take<float4>(2 * (PL + kFp32Pad));
     float4* colrec = cv.take<float4>(2 * (PL + kFp32Pad));
     unsigned long long* key = cv.take<unsigned long long>(PL);
+    Fp32TileParams* desc = cv.take<Fp32TileParams>(1);
+    unsigned long long* counter = cv.take<unsigned long long>(1);
     double* d2 = o_dev ? dist2_out : cv.take<double>(PL);
     int64_t* ix = o_dev ? idx_out : cv.take<int64_t>(PL);
 
@@ -448,21 +455,16 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
         P.g_lo = S.lo;
         P.g_hi = S.hi;
         P.K = K;
-        const int64_t span = 32 * kFp32R;
-        P.nbands = (ndiag + span - 1) / span;
-        int64_t spp = 0;
-        const int64_t npairs = (P.nbands + 1) / 2;
-        for (int64_t p = 0; p < npairs; ++p) {
-            const int64_t l0 = PL - (S.lo + p * span);
-            int64_t t = (l0 + K - 1) / K;
-            const int64_t p2 = P.nbands - 1 - p;
-            if (p2 > p) t += (PL - (S.lo + p2 * span) + K - 1) / K;
-            spp = std::max(spp, t);
-        }
-        P.seg_per_pair = std::max<int64_t>(spp, 1);
+        int64_t ntiles = 0;
+        fp32_tile_plan(PL, S.lo, S.hi, K, kFp32R, P.nbands, P.seg_per_pair, ntiles);
+        P.tile_begin = 0;
         P.key = key;
-        launch_fp32_tiles<kFp32R>(P, 0, npairs * P.seg_per_pair, st);
+        MP_CUDA(ctx, cudaMemcpyAsync(desc, &P, sizeof P, cudaMemcpyHostToDevice, st));
+        MP_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
+        launch_fp32_join<kFp32R>(desc, 1, ntiles, counter, st);
         MP_LAUNCHED(ctx);
+        // the descriptor copy above reads host stack memory: finish it before returning
+        MP_CUDA(ctx, cudaStreamSynchronize(st));
     }
     mark(ctx, 2, st);
     finalize_fp32_kernel<<<grid_for(PL), kThreads, 0, st>>>(key, PL, (double)m, Apad, mean, norm, 0,

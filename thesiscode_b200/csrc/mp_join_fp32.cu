@@ -26,6 +26,8 @@
 //
 // Reference semantics kept: strict improvement over the initial score -1
 // (u < 1 + 1/m), NaN never wins (a zero-variance window has nn = NaN).
+#include <algorithm>
+
 #include "mp_common.cuh"
 #include "mp_kernels.h"
 
@@ -308,7 +310,8 @@ constexpr int fp32_smem_bytes() {
 
 template <int R>
 __global__ void __launch_bounds__(32 * kFp32WarpsPerBlock, MPGPU_FP32_MIN_BLOCKS)
-    fp32_tile_kernel(const Fp32TileParams P, int64_t first_tile, int64_t count) {
+    fp32_join_kernel(const Fp32TileParams* __restrict__ series, int nseries, int64_t total,
+                     unsigned long long* __restrict__ counter) {
     extern __shared__ __align__(128) char smem_fp32[];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -317,43 +320,84 @@ __global__ void __launch_bounds__(32 * kFp32WarpsPerBlock, MPGPU_FP32_MIN_BLOCKS
                   w * kRowKeySlots;
     char* cring = smem_fp32 + kFp32WarpsPerBlock * (kRecRingBytes + kRowKeySlots * (int)sizeof(float)) +
                   w * 4 * 32 * R;
-    const int64_t t = (int64_t)blockIdx.x * kFp32WarpsPerBlock + w;
-    if (t >= count) return;
-    // tile t -> band pair p, slot s; the pair's bands k and nbands-1-k have
-    // nearly complementary lengths, so pairs carry nearly equal tile counts.
-    // Consecutive tiles are consecutive column segments of one band: tiles
-    // running together touch disjoint columns and rows.
-    const int64_t tt = first_tile + t;
-    const int64_t p = tt / P.seg_per_pair;
-    int64_t s = tt % P.seg_per_pair;
-    const int64_t span = 32 * R;
-    const int64_t nseg0 = (P.PL - (P.g_lo + p * span) + P.K - 1) / P.K;
-    if (s < nseg0) {
-        tile_fp32<R>(P, p, s, lane, ring, rring, cring);
-        return;
+    // Persistent warps: each takes the next tile number from one global
+    // counter until the tile space is exhausted (no waiting on anything).
+    for (;;) {
+        unsigned long long t0 = 0;
+        if (lane == 0) t0 = atomicAdd(counter, 1ull);
+        const int64_t tt = (int64_t)__shfl_sync(kFullMask, t0, 0);
+        if (tt >= total) break;
+        // the series owning tile tt: last descriptor with tile_begin <= tt
+        int lo = 0, hi = nseries - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (series[mid].tile_begin <= tt) lo = mid;
+            else hi = mid - 1;
+        }
+        const Fp32TileParams P = series[lo];
+        // local tile -> band pair p, slot s; the pair's bands k and nbands-1-k
+        // have nearly complementary lengths, so pairs carry nearly equal tile
+        // counts.  Consecutive tiles are consecutive column segments of one
+        // band: tiles running together touch disjoint columns and rows.
+        const int64_t lt = tt - P.tile_begin;
+        const int64_t p = lt / P.seg_per_pair;
+        int64_t s = lt % P.seg_per_pair;
+        const int64_t span = 32 * R;
+        const int64_t nseg0 = (P.PL - (P.g_lo + p * span) + P.K - 1) / P.K;
+        if (s < nseg0) {
+            tile_fp32<R>(P, p, s, lane, ring, rring, cring);
+            continue;
+        }
+        s -= nseg0;
+        const int64_t p2 = P.nbands - 1 - p;
+        if (p2 <= p) continue;
+        const int64_t nseg1 = (P.PL - (P.g_lo + p2 * span) + P.K - 1) / P.K;
+        if (s < nseg1) tile_fp32<R>(P, p2, s, lane, ring, rring, cring);
     }
-    s -= nseg0;
-    const int64_t p2 = P.nbands - 1 - p;
-    if (p2 <= p) return;
-    const int64_t nseg1 = (P.PL - (P.g_lo + p2 * span) + P.K - 1) / P.K;
-    if (s < nseg1) tile_fp32<R>(P, p2, s, lane, ring, rring, cring);
 }
 
 }  // namespace
 
-template <int R>
-void launch_fp32_tiles(const Fp32TileParams& P, int64_t first_tile, int64_t count, cudaStream_t s) {
-    const int64_t blocks = (count + kFp32WarpsPerBlock - 1) / kFp32WarpsPerBlock;
-    constexpr int smem = fp32_smem_bytes<R>();
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(fp32_tile_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        configured = true;
+void fp32_tile_plan(int64_t PL, int64_t g_lo, int64_t g_hi, int64_t K, int R, int64_t& nbands,
+                    int64_t& seg_per_pair, int64_t& ntiles) {
+    const int64_t span = 32 * R;
+    const int64_t ndiag = g_hi > g_lo ? g_hi - g_lo : 0;
+    nbands = (ndiag + span - 1) / span;
+    const int64_t npairs = (nbands + 1) / 2;
+    int64_t spp = 0;
+    for (int64_t p = 0; p < npairs; ++p) {
+        int64_t t = (PL - (g_lo + p * span) + K - 1) / K;
+        const int64_t p2 = nbands - 1 - p;
+        if (p2 > p) t += (PL - (g_lo + p2 * span) + K - 1) / K;
+        spp = std::max(spp, t);
     }
-    if (blocks > 0)
-        fp32_tile_kernel<R><<<(unsigned)blocks, 32 * kFp32WarpsPerBlock, smem, s>>>(P, first_tile, count);
+    seg_per_pair = std::max<int64_t>(spp, 1);
+    ntiles = npairs * seg_per_pair;
 }
 
-template void launch_fp32_tiles<8>(const Fp32TileParams&, int64_t, int64_t, cudaStream_t);
+template <int R>
+void configure_fp32_join() {
+    cudaFuncSetAttribute(fp32_join_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         fp32_smem_bytes<R>());
+}
+
+template <int R>
+void launch_fp32_join(const Fp32TileParams* series_dev, int nseries, int64_t total,
+                      unsigned long long* counter, cudaStream_t s) {
+    static bool configured = false;
+    if (!configured) {
+        configure_fp32_join<R>();
+        configured = true;
+    }
+    const int64_t want = (total + kFp32WarpsPerBlock - 1) / kFp32WarpsPerBlock;
+    const int64_t blocks = std::min<int64_t>(want, 148 * MPGPU_FP32_MIN_BLOCKS);
+    if (blocks > 0)
+        fp32_join_kernel<R><<<(unsigned)blocks, 32 * kFp32WarpsPerBlock, fp32_smem_bytes<R>(), s>>>(
+            series_dev, nseries, total, counter);
+}
+
+template void launch_fp32_join<8>(const Fp32TileParams*, int, int64_t, unsigned long long*,
+                                  cudaStream_t);
+template void configure_fp32_join<8>();
 
 }  // namespace mpgpu

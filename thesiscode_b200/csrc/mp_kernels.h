@@ -5,7 +5,12 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+struct mp_context;
+
 namespace mpgpu {
+
+// Memory budget of a context (0 = none); defined with the context in mp_capi.cu.
+size_t ctx_budget(const mp_context* ctx);
 
 // ---- preparation (mp_prep.cu) ----------------------------------------------
 __global__ void ref_prefix_kernel(const double* A, int64_t n, double* cs, double* cs2);
@@ -52,6 +57,8 @@ template <int R>
 void launch_fp64_band(const Fp64BandParams& P, cudaStream_t s);
 
 // ---- FP32 re-anchored tile join (mp_join_fp32.cu) ---------------------------
+// One series of a (batched) join.  Its tiles are numbered
+// [tile_begin, tile_begin + npairs * seg_per_pair) in the launch's tile space.
 struct Fp32TileParams {
     const float4* rowrec;  // pairs (x[j], x[j+H]) of df, dg, nn; 2 float4 per row
     const float4* colrec;  // duplicated, negated column terms; 2 float4 per column
@@ -62,10 +69,19 @@ struct Fp32TileParams {
     int64_t K;             // columns per tile = re-anchor interval
     int64_t nbands;        // bands of 32R diagonals
     int64_t seg_per_pair;  // tiles per band pair (k, nbands-1-k), max over pairs
+    int64_t tile_begin;    // first tile of this series in the launch
     unsigned long long* key;  // [PL] (ordered u << 32 | neighbour), min-merged
 };
+// Persistent launch over `nseries` descriptors (device array) holding `total`
+// tiles; warps take tiles from *counter (zeroed by the caller beforehand).
 template <int R>
-void launch_fp32_tiles(const Fp32TileParams& P, int64_t first_tile, int64_t count, cudaStream_t s);
+void launch_fp32_join(const Fp32TileParams* series_dev, int nseries, int64_t total,
+                      unsigned long long* counter, cudaStream_t s);
+template <int R>
+void configure_fp32_join();
+// Tile count and seg_per_pair of one series (host helper).
+void fp32_tile_plan(int64_t PL, int64_t g_lo, int64_t g_hi, int64_t K, int R, int64_t& nbands,
+                    int64_t& seg_per_pair, int64_t& ntiles);
 
 // ---- finalisation (mp_finalize.cu) -------------------------------------------
 __global__ void init_keys_kernel(unsigned long long* k, int64_t count, unsigned long long v);
