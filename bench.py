@@ -380,13 +380,75 @@ def run_ours(args, world):
     ctx.close()
 
 
+def run_batch_workload(args):
+    """Workload c4: 4,096 FP32-input walks (lengths log-uniform in [2048,
+    262144], m in {64, 128, 256}) solved by one persistent, graph-captured
+    launch per step; tile widths from the autotuner table."""
+    import torch
+
+    import thesiscode_b200 as mp
+    import thesiscode_b200.workloads as wl
+    data = wl.c4(args.c4_count)
+    lens = [x.size for x, _ in data]
+    ms = [m for _, m in data]
+    ctx = mp.Context(0)
+    b = mp.Batch(ctx, lens, ms, None, input_f32=True)
+    stream = torch.cuda.Stream()
+    b.upload([x for x, _ in data], stream.cuda_stream)
+    for _ in range(args.warmup):
+        b.launch(stream.cuda_stream)
+    stream.synchronize()
+    evs = []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.launch(stream.cuda_stream)
+            e1.record(stream)
+            evs.append((e0, e1))
+        stream.synchronize()
+    ms_step = float(np.mean([a.elapsed_time(c) for a, c in evs]))
+    t0 = time.perf_counter()
+    b.run([x for x, _ in data], stream.cuda_stream)
+    e2e_s = time.perf_counter() - t0
+    line = {"metric": "batched self-join cells/s (c4, one persistent graph-captured launch)",
+            "value": b.cells / (ms_step * 1e-3), "unit": "cells/s", "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"c4: {len(data)} FP32 random walks, lengths log-uniform "
+                                   f"[2048, 262144], m in {{64,128,256}}, seed 3",
+                       "series": len(data), "samples": int(sum(lens)), "cells": b.cells,
+                       "tiles": b.tiles, "launches_per_step": b.launch_count},
+            "e2e": {"value": b.cells / e2e_s, "unit": "cells/s",
+                    "h2d_bytes_per_step": 4 * int(sum(lens)),
+                    "d2h_bytes_per_step": 16 * int(sum(l - m + 1 for l, m in zip(lens, ms)))},
+            "gpu_launches": b.launch_count * args.steps, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    b.close()
+    ctx.close()
+
+
+def run_serving_workload(args):
+    """Workload c5: Poisson request streams at several rates against the
+    continuous-batching server; p50/p99 latency and admitted cells/s."""
+    from thesiscode_b200.serve import run_stream
+    for rate in args.rates:
+        r = run_stream(rate, args.serve_seconds, slots=args.slots)
+        r["metric"] = "serving p50/p99 solve latency (c5)"
+        print(json.dumps(r), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["c2", "c1"], default="c2")
+    ap.add_argument("--workload", choices=["c2", "c1", "c4", "c5"], default="c2")
+    ap.add_argument("--c4-count", type=int, default=4096)
+    ap.add_argument("--rates", type=float, nargs="+", default=[10, 30, 100, 300])
+    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--slots", type=int, default=4)
     ap.add_argument("--reanchor-k", type=int, default=1024)
     ap.add_argument("--fp64-steps", type=int, default=3)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
@@ -395,6 +457,12 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         run_reference_arm(args, world)
+        return
+    if args.workload == "c4":
+        run_batch_workload(args)
+        return
+    if args.workload == "c5":
+        run_serving_workload(args)
         return
     import torch
     import torch.distributed as dist

@@ -150,6 +150,30 @@ int mp_batch_download(mp_batch* b, double* const* dist2_out, int64_t* const* idx
 int mp_batch_run(mp_batch* b, const void* const* series, double* const* dist2_out,
                  int64_t* const* idx_out, void* stream);
 
+/*
+ * Request server (no counterpart in the reference).  Continuous batching of
+ * independent self-joins: requests are admitted in arrival order as soon as one
+ * of `slots` workers is free and the device memory they need (scratch +
+ * resident result, see mp_selfjoin_scratch_bytes) fits in mem_budget_bytes;
+ * admitted requests run concurrently on their own streams.  A finished profile
+ * stays on the device until mp_server_collect copies it out (and frees it).
+ * A request larger than the whole budget is rejected (MP_ERR_BUDGET).
+ *   mp_server_submit   copies the host series, returns a ticket, never blocks
+ *   mp_server_poll     1 when finished (status set), 0 while pending
+ *   mp_server_collect  waits for the ticket, copies d2/idx (may be NULL), frees;
+ *                      latency = submission to finish, queue = submission to start
+ */
+typedef struct mp_server mp_server;
+int mp_server_create(int device, size_t mem_budget_bytes, int slots, int precision,
+                     int64_t reanchor_k, mp_server** out);
+int mp_server_submit(mp_server* s, const double* A, int64_t n, int64_t m, int64_t* ticket);
+int mp_server_poll(mp_server* s, int64_t ticket, int* status);
+int mp_server_collect(mp_server* s, int64_t ticket, double* dist2_out, int64_t* idx_out,
+                      double* latency_s, double* queue_s);
+int mp_server_stats(mp_server* s, int64_t* completed, int64_t* rejected, int64_t* waiting,
+                    int64_t* running, double* cells, size_t* bytes_in_use);
+int mp_server_destroy(mp_server* s);
+
 /* FMA throughput of this device's CUDA-core pipes in FLOP/s (2 per FMA),
  * measured with independent FMA chains: which = 0 FP32 (FFMA), 1 FP32 (f32x2
  * FFMA2), 2 FP64 (DFMA).  The join kernels' compute roofline uses it. */

@@ -1,0 +1,75 @@
+"""Continuous-batching server: results are identical alone and in the mix
+(requests admitted while others run, overlapping on the device), admission
+respects the memory budget, oversized requests are rejected."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import thesiscode_b200 as mp
+from thesiscode_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(seed, count):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(np.exp(rng.uniform(np.log(2000), np.log(60000))))
+        m = int(rng.choice([32, 64, 128, 256]))
+        out.append((workloads.random_walk(n, 100 + i), m))
+    return out
+
+
+def test_same_result_alone_and_in_the_mix(oracle):
+    reqs = _requests(7, 6)
+    others = _requests(8, 10)
+    srv = mp.Server(0, 8 << 30, slots=4)
+    alone = []
+    for x, m in reqs:
+        t, rc = srv.submit(x, m)
+        assert rc == mp.MP_OK
+        rc, p, lat, _ = srv.collect(t)
+        assert rc == mp.MP_OK and lat > 0
+        alone.append(p)
+    # now interleaved with other traffic, all submitted at once
+    tickets = []
+    for i in range(max(len(reqs), len(others))):
+        if i < len(others):
+            tickets.append(("o", srv.submit(*others[i])[0]))
+        if i < len(reqs):
+            tickets.append(("r", srv.submit(*reqs[i])[0]))
+    mixed = [srv.collect(t)[1] for kind, t in tickets if kind == "r"]
+    # the other requests' profiles stay resident (and counted) until collected
+    assert srv.stats()["bytes_in_use"] > 0
+    for kind, t in tickets:
+        if kind == "o":
+            assert srv.collect(t, want_profile=False)[0] == mp.MP_OK
+    for a, b, (x, m) in zip(alone, mixed, reqs):
+        assert np.array_equal(a.dist2, b.dist2) and np.array_equal(a.index, b.index)
+        d2, _ = oracle.selfjoin(x, m)
+        rel = np.abs(np.sqrt(np.abs(b.dist2)) - np.sqrt(d2)) / np.sqrt(d2)
+        assert rel.max() <= 1e-4
+    st = srv.stats()
+    assert st["completed"] == len(reqs) * 2 + len(others) and st["bytes_in_use"] == 0
+    srv.close()
+
+
+def test_admission_by_memory_budget():
+    x = workloads.random_walk(200_000, 1)
+    need = mp.load_library().mp_selfjoin_scratch_bytes(x.size, 128, mp.FP32_REANCHOR)
+    srv = mp.Server(0, int(need * 1.2) + (16 << 20), slots=4)  # room for one at a time
+    ts = [srv.submit(x, 128)[0] for _ in range(3)]
+    st = srv.stats()
+    assert st["running"] <= 1 and st["waiting"] + st["running"] + st["completed"] >= 1
+    res = [srv.collect(t) for t in ts]
+    assert all(r[0] == mp.MP_OK for r in res)
+    assert np.array_equal(res[0][1].dist2, res[2][1].dist2)
+    # a request larger than the whole budget is rejected at submission
+    big = workloads.random_walk(2_000_000, 2)
+    t, rc = srv.submit(big, 256)
+    assert rc == mp.MP_ERR_BUDGET
+    assert srv.collect(t, want_profile=False)[0] == mp.MP_ERR_BUDGET
+    assert srv.stats()["rejected"] == 1
+    srv.close()

@@ -47,7 +47,8 @@ EXPORTED_SYMBOLS = (
     "mp_run_algorithm", "mp_set_phase_timing", "mp_last_phase_ms", "mp_measure_fma_peak",
     "mp_batch_create", "mp_batch_destroy", "mp_batch_cells", "mp_batch_tiles",
     "mp_batch_launch_count", "mp_batch_upload", "mp_batch_launch", "mp_batch_download",
-    "mp_batch_run",
+    "mp_batch_run", "mp_server_create", "mp_server_submit", "mp_server_poll", "mp_server_collect",
+    "mp_server_stats", "mp_server_destroy",
 )
 
 
@@ -104,6 +105,16 @@ def load_library() -> ctypes.CDLL:
     L.mp_batch_launch.argtypes = [_P, _P]
     L.mp_batch_download.argtypes = [_P, _P, _P, _P]
     L.mp_batch_run.argtypes = [_P, _P, _P, _P, _P]
+    L.mp_server_create.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, _i64,
+                                   ctypes.POINTER(_P)]
+    L.mp_server_submit.argtypes = [_P, _P, _i64, _i64, ctypes.POINTER(_i64)]
+    L.mp_server_poll.argtypes = [_P, _i64, ctypes.POINTER(ctypes.c_int)]
+    L.mp_server_collect.argtypes = [_P, _i64, _P, _P, ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_double)]
+    L.mp_server_stats.argtypes = [_P, ctypes.POINTER(_i64), ctypes.POINTER(_i64),
+                                  ctypes.POINTER(_i64), ctypes.POINTER(_i64),
+                                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_size_t)]
+    L.mp_server_destroy.argtypes = [_P]
     L.mp_list_algorithms.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     L.mp_run_algorithm.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -336,6 +347,68 @@ class Batch:
         self.upload(series, stream)
         self.launch(stream)
         return self.download(stream)
+
+
+class Server:
+    """Continuous-batching request server (mp_server_*): submit self-joins,
+    collect profiles; admission by device-memory budget, `slots` concurrent
+    workers each on its own stream."""
+
+    def __init__(self, device: int = 0, mem_budget_bytes: int = 8 << 30, slots: int = 4,
+                 precision: int = FP32_REANCHOR, reanchor_k: int = 1024):
+        self._L = load_library()
+        h = _P()
+        rc = self._L.mp_server_create(device, mem_budget_bytes, slots, precision, reanchor_k,
+                                      ctypes.byref(h))
+        if rc != MP_OK:
+            raise MpError(rc, status_string(rc))
+        self._h = h
+        self._pl = {}
+
+    def submit(self, A, m: int) -> tuple[int, int]:
+        """Returns (ticket, status); status MP_ERR_BUDGET means rejected."""
+        A = np.ascontiguousarray(A, dtype=np.float64)
+        t = _i64()
+        rc = self._L.mp_server_submit(self._h, A.ctypes.data, A.size, m, ctypes.byref(t))
+        if rc not in (MP_OK, MP_ERR_BUDGET):
+            raise MpError(rc, status_string(rc))
+        self._pl[t.value] = A.size - m + 1
+        return t.value, rc
+
+    def done(self, ticket: int) -> bool:
+        st = ctypes.c_int()
+        return self._L.mp_server_poll(self._h, ticket, ctypes.byref(st)) == 1
+
+    def collect(self, ticket: int, want_profile: bool = True):
+        """Waits; returns (status, Profile or None, latency_s, queue_s)."""
+        PL = self._pl.pop(ticket)
+        d2 = np.empty(PL) if want_profile else None
+        ix = np.empty(PL, dtype=np.int64) if want_profile else None
+        lat, que = ctypes.c_double(), ctypes.c_double()
+        rc = self._L.mp_server_collect(self._h, ticket, _ptr(d2), _ptr(ix), ctypes.byref(lat),
+                                       ctypes.byref(que))
+        prof = Profile(d2, ix) if (want_profile and rc == MP_OK) else None
+        return rc, prof, lat.value, que.value
+
+    def stats(self) -> dict:
+        c, r, w, u = _i64(), _i64(), _i64(), _i64()
+        cells = ctypes.c_double()
+        used = ctypes.c_size_t()
+        self._L.mp_server_stats(self._h, ctypes.byref(c), ctypes.byref(r), ctypes.byref(w),
+                                ctypes.byref(u), ctypes.byref(cells), ctypes.byref(used))
+        return {"completed": c.value, "rejected": r.value, "waiting": w.value,
+                "running": u.value, "cells": cells.value, "bytes_in_use": used.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.mp_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def cells(n: int, m: int, diag_lo: int = 0, diag_hi: int = 0, excl: int = -1) -> int:

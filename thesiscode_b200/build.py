@@ -23,11 +23,14 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SOURCES = ["mp_prep.cu", "mp_join_fp64.cu", "mp_join_fp32.cu", "mp_finalize.cu",
                 "mp_capi.cu", "mp_calib.cu", "mp_batch.cu"]
-HOST_SOURCES = ["host/matprof_algo.cpp", "host/gpu_variants.cpp", "host/profile_io.cpp"]
+HOST_SOURCES = ["host/matprof_algo.cpp", "host/gpu_variants.cpp", "host/profile_io.cpp",
+                "host/mp_server.cpp"]
 CLI_SOURCES = ["host/main.cpp"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", *ARCH,
               f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}"]
-CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}"]
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}",
+             f"-I{os.path.join(CUDA_HOME, 'include')}"]
 
 
 def _stale(target: str, deps: list[str]) -> bool:

@@ -1,0 +1,283 @@
+// Self-join request server: continuous batching of independent self-joins.
+//
+// Requests are admitted in arrival order as soon as a worker slot is free and
+// the device memory they need (scratch + their resident result) fits in the
+// server's budget; admitted requests run concurrently, each worker on its own
+// CUDA stream and context, so the GPU overlaps their kernels.  A finished
+// profile stays in device memory until the client collects it, and its memory
+// counts against the budget until then.  A request larger than the whole
+// budget is rejected at submission.  No counterpart in the reference (one
+// join per process there).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "mpgpu.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    int64_t id = 0;
+    std::vector<double> series;
+    int64_t m = 0, PL = 0;
+    size_t need = 0;       // device bytes while running: scratch + resident result
+    size_t accounted = 0;  // bytes of this request currently counted in in_use
+    Clock::time_point submitted, started, finished;
+    int status = -1;  // -1 pending, >= 0 final status
+    double* d_d2 = nullptr;
+    int64_t* d_idx = nullptr;
+    bool collected = false;
+};
+
+}  // namespace
+
+struct mp_server {
+    int device = 0;
+    size_t budget = 0;
+    int precision = MP_PREC_FP32_REANCHOR;
+    int64_t reanchor_k = 0;
+    std::mutex mu;
+    std::condition_variable cv_work;  // workers wait for admissions
+    std::condition_variable cv_done;  // clients wait for completions
+    std::deque<int64_t> waiting;      // submitted, not admitted (FIFO)
+    std::deque<int64_t> admitted;     // admitted, not started
+    std::unordered_map<int64_t, std::unique_ptr<Request>> reqs;
+    size_t in_use = 0;  // bytes of admitted + resident requests
+    int free_slots = 0;
+    int64_t next_id = 1;
+    bool stop = false;
+    std::vector<std::thread> workers;
+    // statistics
+    int64_t completed = 0, rejected = 0;
+    double cells_done = 0.0;
+};
+
+namespace {
+
+size_t result_bytes(int64_t PL) { return 16 * (size_t)PL + 512; }
+
+double cells_of(int64_t n, int64_t m) {
+    const double L = (double)std::max<int64_t>(n - m + 1 - m / 4 - 1, 0);
+    return L * (L + 1) / 2;
+}
+
+// Moves waiting requests to `admitted` while slots and memory allow (FIFO:
+// the head blocks the queue, so a large request is never starved).
+void admit_locked(mp_server* s) {
+    while (!s->waiting.empty() && s->free_slots > 0) {
+        Request* r = s->reqs[s->waiting.front()].get();
+        if (s->in_use + r->need > s->budget && s->in_use > 0) break;
+        s->waiting.pop_front();
+        s->in_use += r->need;
+        r->accounted = r->need;
+        --s->free_slots;
+        s->admitted.push_back(r->id);
+        s->cv_work.notify_one();
+    }
+}
+
+void worker_main(mp_server* s) {
+    cudaSetDevice(s->device);
+    cudaStream_t st;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    mp_context* ctx = nullptr;
+    mp_context_create(s->device, 0, &ctx);
+    for (;;) {
+        Request* r = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_work.wait(lk, [&] { return s->stop || !s->admitted.empty(); });
+            if (s->stop && s->admitted.empty()) break;
+            r = s->reqs[s->admitted.front()].get();
+            s->admitted.pop_front();
+            r->started = Clock::now();
+        }
+        const int64_t n = (int64_t)r->series.size(), PL = r->PL;
+        int rc = ctx ? MP_OK : MP_ERR_NO_DEVICE;
+        if (rc == MP_OK && (cudaMallocAsync((void**)&r->d_d2, 8 * PL, st) != cudaSuccess ||
+                            cudaMallocAsync((void**)&r->d_idx, 8 * PL, st) != cudaSuccess)) {
+            cudaGetLastError();
+            rc = MP_ERR_OUT_OF_MEMORY;
+        }
+        if (rc == MP_OK)
+            rc = mp_selfjoin(ctx, r->series.data(), n, r->m, -1, s->precision, s->reanchor_k, 0, 0,
+                             0, r->d_d2, r->d_idx, st);
+        if (rc != MP_OK) {
+            if (r->d_d2) cudaFreeAsync(r->d_d2, st);
+            if (r->d_idx) cudaFreeAsync(r->d_idx, st);
+            r->d_d2 = nullptr;
+            r->d_idx = nullptr;
+            cudaStreamSynchronize(st);
+        }
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            r->finished = Clock::now();
+            r->status = rc;
+            r->series.clear();
+            r->series.shrink_to_fit();
+            // scratch is released; a resident result keeps its share
+            const size_t keep = (rc == MP_OK) ? result_bytes(PL) : 0;
+            s->in_use -= r->accounted - keep;
+            r->accounted = keep;
+            ++s->free_slots;
+            if (rc == MP_OK) {
+                ++s->completed;
+                s->cells_done += cells_of(n, r->m);
+            }
+            admit_locked(s);
+        }
+        s->cv_done.notify_all();
+    }
+    if (ctx) mp_context_destroy(ctx);
+    cudaStreamDestroy(st);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mp_server_create(int device, size_t mem_budget_bytes, int slots, int precision,
+                     int64_t reanchor_k, mp_server** out) {
+    if (!out || slots < 1 || mem_budget_bytes == 0) return MP_ERR_INVALID_ARG;
+    if (precision != MP_PREC_FP64 && precision != MP_PREC_FP32_REANCHOR) return MP_ERR_INVALID_ARG;
+    mp_context* probe = nullptr;
+    const int rc = mp_context_create(device, 0, &probe);
+    if (rc != MP_OK) return rc;
+    mp_context_destroy(probe);
+    mp_server* s = new mp_server();
+    s->device = device;
+    s->budget = mem_budget_bytes;
+    s->precision = precision;
+    s->reanchor_k = reanchor_k;
+    s->free_slots = slots;
+    for (int i = 0; i < slots; ++i) s->workers.emplace_back(worker_main, s);
+    *out = s;
+    return MP_OK;
+}
+
+int mp_server_submit(mp_server* s, const double* A, int64_t n, int64_t m, int64_t* ticket) {
+    if (!s || !A || !ticket || m < 2 || n < m) return MP_ERR_INVALID_ARG;
+    auto r = std::make_unique<Request>();
+    r->series.assign(A, A + n);
+    r->m = m;
+    r->PL = n - m + 1;
+    r->need = mp_selfjoin_scratch_bytes(n, m, s->precision) + result_bytes(n - m + 1);
+    r->submitted = Clock::now();
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->id = s->next_id++;
+    *ticket = r->id;
+    if (r->need > s->budget) {
+        r->status = MP_ERR_BUDGET;
+        r->finished = r->submitted;
+        ++s->rejected;
+        s->reqs[r->id] = std::move(r);
+        return MP_ERR_BUDGET;
+    }
+    const int64_t id = r->id;
+    s->reqs[id] = std::move(r);
+    s->waiting.push_back(id);
+    admit_locked(s);
+    return MP_OK;
+}
+
+// 0 = pending, 1 = finished (status then holds the result's status).
+int mp_server_poll(mp_server* s, int64_t ticket, int* status) {
+    if (!s) return MP_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return MP_ERR_INVALID_ARG;
+    if (status) *status = it->second->status;
+    return it->second->status >= 0 ? 1 : 0;
+}
+
+int mp_server_collect(mp_server* s, int64_t ticket, double* dist2_out, int64_t* idx_out,
+                      double* latency_s, double* queue_s) {
+    if (!s) return MP_ERR_INVALID_ARG;
+    Request* r = nullptr;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        auto it = s->reqs.find(ticket);
+        if (it == s->reqs.end()) return MP_ERR_INVALID_ARG;
+        r = it->second.get();
+        s->cv_done.wait(lk, [&] { return r->status >= 0; });
+        if (r->collected) return MP_ERR_INVALID_ARG;
+        r->collected = true;
+    }
+    int rc = r->status;
+    if (latency_s)
+        *latency_s = std::chrono::duration<double>(r->finished - r->submitted).count();
+    if (queue_s)
+        *queue_s = rc == MP_ERR_BUDGET
+                       ? 0.0
+                       : std::chrono::duration<double>(r->started - r->submitted).count();
+    if (r->d_d2) {
+        // a private stream: no device-wide synchronisation while others run
+        cudaSetDevice(s->device);
+        cudaStream_t st;
+        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        if (rc == MP_OK) {
+            if ((dist2_out &&
+                 cudaMemcpyAsync(dist2_out, r->d_d2, 8 * r->PL, cudaMemcpyDeviceToHost, st) != cudaSuccess) ||
+                (idx_out &&
+                 cudaMemcpyAsync(idx_out, r->d_idx, 8 * r->PL, cudaMemcpyDeviceToHost, st) != cudaSuccess)) {
+                cudaGetLastError();
+                rc = MP_ERR_CUDA;
+            }
+        }
+        cudaFreeAsync(r->d_d2, st);
+        cudaFreeAsync(r->d_idx, st);
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->in_use -= r->accounted;
+        s->reqs.erase(ticket);
+        admit_locked(s);
+    }
+    return rc;
+}
+
+int mp_server_stats(mp_server* s, int64_t* completed, int64_t* rejected, int64_t* waiting,
+                    int64_t* running, double* cells, size_t* bytes_in_use) {
+    if (!s) return MP_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (completed) *completed = s->completed;
+    if (rejected) *rejected = s->rejected;
+    if (waiting) *waiting = (int64_t)s->waiting.size();
+    if (running) *running = (int64_t)s->workers.size() - s->free_slots;
+    if (cells) *cells = s->cells_done;
+    if (bytes_in_use) *bytes_in_use = s->in_use;
+    return MP_OK;
+}
+
+int mp_server_destroy(mp_server* s) {
+    if (!s) return MP_ERR_INVALID_ARG;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->waiting.clear();
+    }
+    s->cv_work.notify_all();
+    for (auto& t : s->workers) t.join();
+    cudaSetDevice(s->device);
+    for (auto& kv : s->reqs) {
+        if (kv.second->d_d2) cudaFree(kv.second->d_d2);
+        if (kv.second->d_idx) cudaFree(kv.second->d_idx);
+    }
+    delete s;
+    return MP_OK;
+}
+
+}  // extern "C"
