@@ -174,6 +174,43 @@ int mp_server_stats(mp_server* s, int64_t* completed, int64_t* rejected, int64_t
                     int64_t* running, double* cells, size_t* bytes_in_use);
 int mp_server_destroy(mp_server* s);
 
+/*
+ * Allocation-free FP32 self-join.  No counterpart in the reference (which
+ * allocates its buffers per run); added for callers that must not allocate
+ * device memory: a host framework that owns the whole GPU through its own
+ * memory pool and forbids other allocators, or a latency-critical path where
+ * cudaMalloc/cudaFree (which can synchronise the device) are not allowed.
+ *
+ * Same arithmetic, kernels and results as mp_selfjoin with
+ * MP_PREC_FP32_REANCHOR over all diagonals, but its scratch is a fixed
+ * device array of MPGPU_NOALLOC_SCRATCH_BYTES that every GPU loading this
+ * library holds until the process exits, so n is limited to
+ * MPGPU_NOALLOC_MAX_N samples; longer series return MP_ERR_NOT_SUPPORTED.
+ * No call allocates or frees memory.
+ *
+ *   A_dev        n doubles in device memory of the current device.
+ *   excl         exclusion zone; < 0 selects m/4.
+ *   reanchor_k   columns between FP64 re-anchors (0 = 1024).
+ *   dist2_dev    PL = n - m + 1 doubles (device): squared distances.
+ *   idx_dev      PL int64 (device): neighbour indices.
+ *   stream       cudaStream_t (NULL = legacy default stream).  The call only
+ *                enqueues work: results are ready when the stream reaches
+ *                this point, and A_dev must stay valid until then.
+ *   err/err_len  optional buffer for a one-line error message (may be NULL).
+ *
+ * The first call on a device (the current device at the time of the call)
+ * looks up the scratch's device address and configures the join kernel
+ * there; make that first call before any stream capture.  All calls on a
+ * device share the one scratch array: calls whose work overlaps on the GPU
+ * (other streams, other host threads) race and corrupt each other's results,
+ * so serialise them (one stream, or events between streams).
+ */
+#define MPGPU_NOALLOC_MAX_N 131072
+#define MPGPU_NOALLOC_SCRATCH_BYTES (14u << 20)
+int mp_selfjoin_fp32_noalloc(const double* A_dev, int64_t n, int64_t m, int64_t excl,
+                             int64_t reanchor_k, double* dist2_dev, int64_t* idx_dev,
+                             void* stream, char* err, size_t err_len);
+
 /* FMA throughput of this device's CUDA-core pipes in FLOP/s (2 per FMA),
  * measured with independent FMA chains: which = 0 FP32 (FFMA), 1 FP32 (f32x2
  * FFMA2), 2 FP64 (DFMA).  The join kernels' compute roofline uses it. */

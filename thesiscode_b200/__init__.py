@@ -48,7 +48,7 @@ EXPORTED_SYMBOLS = (
     "mp_batch_create", "mp_batch_destroy", "mp_batch_cells", "mp_batch_tiles",
     "mp_batch_launch_count", "mp_batch_upload", "mp_batch_launch", "mp_batch_download",
     "mp_batch_run", "mp_server_create", "mp_server_submit", "mp_server_poll", "mp_server_collect",
-    "mp_server_stats", "mp_server_destroy",
+    "mp_server_stats", "mp_server_destroy", "mp_selfjoin_fp32_noalloc",
 )
 
 
