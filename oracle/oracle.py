@@ -60,6 +60,7 @@ class Oracle:
         L.orc_selfjoin_fp64.argtypes = [_D, _i64, _i64, _i64, _i64, _i64, _i64, ctypes.c_int,
                                         _D, _L]
         L.orc_pair_d2.argtypes = [_D, _i64, _i64, _i64, _i64]
+        L.orc_cell_scores.argtypes = [_D, _i64, _i64, _i64, _i64, _D, _D, _i64, _L, _L, _D]
         L.orc_pair_d2.restype = ctypes.c_double
         L.orc_cells.argtypes = [_i64, _i64, _i64, _i64]
         L.orc_cells.restype = ctypes.c_double
@@ -101,6 +102,19 @@ class Oracle:
                                               _dptr(A_hor), _dptr(A_vert), m, _dptr(s_hor),
                                               _dptr(mu_hor), _dptr(s_vert), _dptr(mu_vert),
                                               baserow, basecol)
+
+    def cell_scores(self, A, m, cols, rows, blocklen=500, excl=-1, stats=None):
+        """Scores the reference's arithmetic gives cells (cols[k], rows[k]) in a
+        vert_blocked join with this blocklen (cols[k] < rows[k])."""
+        A = np.ascontiguousarray(A, dtype=np.float64)
+        muS, sInv = stats if stats is not None else self.window_stats(A, m)
+        c = np.ascontiguousarray(cols, dtype=np.int64)
+        r = np.ascontiguousarray(rows, dtype=np.int64)
+        out = np.empty(c.size)
+        rc = self.lib.orc_cell_scores(_dptr(A), A.size, m, excl, blocklen, _dptr(muS),
+                                      _dptr(sInv), c.size, _lptr(c), _lptr(r), _dptr(out))
+        assert rc == 0, rc
+        return out
 
     def pair_d2(self, A, m, i, j):
         A = np.ascontiguousarray(A, dtype=np.float64)

@@ -296,6 +296,52 @@ int orc_selfjoin_fp64(const double* A, int64_t n, int64_t m, int64_t excl, int64
     return rc;
 }
 
+/* One cell's score in the reference's arithmetic: the diagonal g = row - col
+ * runs from its first dot product (ScrimpSequOpt.cpp:81-96) through the block
+ * of blocklen diagonals that holds it (ScrimpVertBlocked.cpp:139-142: cut at
+ * excl+1 + k*blocklen, triangle length PL - block start), each cell fused or
+ * separately rounded as its position in that block selects -- the same
+ * per-cell operations as block_core above (kernels.cpp:194-300). */
+int orc_cell_scores(const double* A, int64_t n, int64_t m, int64_t excl, int64_t blocklen,
+                    const double* muS, const double* sInv, int64_t count, const int64_t* col,
+                    const int64_t* row, double* score) {
+    if (m < 2 || n < m || blocklen < 1) return -1;
+    const int64_t PL = n - m + 1;
+    if (excl < 0) excl = m / 4;
+    for (int64_t k = 0; k < count; ++k) {
+        const int64_t c = col[k], r = row[k], g = r - c;
+        if (c < 0 || r >= PL || g < excl + 1) return -2;
+        const int64_t d0 = excl + 1 + ((g - excl - 1) / blocklen) * blocklen;
+        const int64_t dg = g - d0, T = PL - d0;
+        double q;
+        orc_first_qt(A, n, m, g, g + 1, &q);
+        double sc = NAN;
+        for (int64_t j = 0; j <= c; ++j) {
+            const int64_t cnt = blocklen < T - j ? blocklen : T - j;
+            const int64_t nvec = cnt - cnt % 4;
+            const double sh = sInv[j], mh = muS[j], sv = sInv[j + g], mv = muS[j + g];
+            if (dg < nvec) {
+                const double ss = sv * sh;
+                const double mm = mh * mv;
+                sc = fma(q, ss, -mm);
+                double t = fma(A[j + g + m], A[j + m], q);
+                q = fma(-A[j + g], A[j], t);
+            } else {
+                const double ss = sv * sh;
+                const double t1 = q * ss;
+                const double t2 = mv * mh;
+                sc = t1 - t2;
+                const double far = A[j + g + m] * A[j + m];
+                double t = q + far;
+                const double near = A[j + g] * A[j];
+                q = t - near;
+            }
+        }
+        score[k] = sc;
+    }
+    return 0;
+}
+
 double orc_pair_d2(const double* A, int64_t n, int64_t m, int64_t i, int64_t j) {
     if (i < 0 || j < 0 || i + m > n || j + m > n) return NAN;
     long double si = 0, sj = 0;

@@ -51,6 +51,16 @@ void orc_eval_diag_block_triangle(double* prof_colmin, int64_t* idx_colmin, doub
 int orc_selfjoin_fp64(const double* A, int64_t n, int64_t m, int64_t excl, int64_t blocklen,
                       int64_t diag_lo, int64_t diag_hi, int nthreads, double* d2, int64_t* idx);
 
+/* Scores that the reference's arithmetic gives the cells (col[k], row[k]),
+ * col < row, row - col > excl, in a vert_blocked join with this blocklen:
+ * the cell's diagonal is run from its first dot product with the fused or
+ * separately rounded operations its place in its block selects.  muS/sInv
+ * from orc_window_stats.  Cost O(col[k]) per cell.  Used to judge whether two
+ * candidate neighbours tie in the reference's own values. */
+int orc_cell_scores(const double* A, int64_t n, int64_t m, int64_t excl, int64_t blocklen,
+                    const double* muS, const double* sInv, int64_t count, const int64_t* col,
+                    const int64_t* row, double* score);
+
 /* Squared z-normalised distance between windows i and j, evaluated in long
  * double with per-window centring (an accuracy yardstick, not the reference
  * arithmetic).  Returns NaN for a window of zero variance. */

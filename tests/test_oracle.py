@@ -143,3 +143,40 @@ def test_restatement_vs_reference_sources_random(oracle):
         d2b, ib, _ = ref.vert_blocked(x, m, blocklen=B, shuffle=False)
         assert np.array_equal(d2a, d2b), trial
         assert np.array_equal(ia, ib), trial
+
+
+def _check_cell_scores(oracle, x, m, B, d2, ix):
+    PL = x.size - m + 1
+    i = np.arange(PL)
+    ok = d2 < 2.0 * m + 2.0  # windows some cell improved
+    s = oracle.cell_scores(x, m, np.minimum(i, ix)[ok], np.maximum(i, ix)[ok], blocklen=B)
+    assert ok.any()
+    assert np.array_equal(2.0 * m - 2.0 * s, d2[ok])
+
+
+def test_cell_scores_reproduce_profile_values(oracle):
+    """A window's profile value is the score of the cell its index names, so
+    recomputing that one cell in the reference's arithmetic must give the
+    value bit for bit -- also for series far from zero, where the recurrence's
+    rounding dominates."""
+    rng = np.random.default_rng(17)
+    for trial in range(4):
+        n = int(rng.integers(500, 4000))
+        m = int(rng.integers(8, 100))
+        x = np.cumsum(rng.standard_normal(n)) * float(rng.choice([1.0, 200.0]))
+        x += float(rng.choice([0.0, 1e4]))
+        B = int(rng.choice([5, 64, 500]))
+        d2, ix = oracle.selfjoin(x, m, blocklen=B)
+        _check_cell_scores(oracle, x, m, B, d2, ix)
+
+
+def test_cell_scores_vs_reference_sources(oracle):
+    ref = _ref_or_skip()
+    rng = np.random.default_rng(19)
+    for trial in range(4):
+        n = int(rng.integers(500, 4000))
+        m = int(rng.integers(8, 100))
+        x = np.cumsum(rng.standard_normal(n)) + float(rng.choice([0.0, 1e4]))
+        B = int(rng.choice([5, 64, 500]))
+        d2, ix, _ = ref.vert_blocked(x, m, blocklen=B, shuffle=True)
+        _check_cell_scores(oracle, x, m, B, d2, ix)

@@ -115,6 +115,15 @@ bool on_device(const void* p) {
     return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
+// Lower end 2^(t-64) of the FP64 index key's distance range, as a bit
+// pattern, with 2^t > 2m + 2 >= every half squared distance m - score of a
+// candidate whose correlation is at least -1 (idx_key_f64).
+long long key_vlo_bits(int64_t m) {
+    int t = 1;
+    while (t < 62 && std::ldexp(1.0, t) <= 2.0 * (double)m + 2.0) ++t;
+    return (long long)(1023 + t - 64) << 52;
+}
+
 int bits_for(uint64_t maxval) {
     int b = 1;
     while (b < 63 && (1ull << b) <= maxval) ++b;
@@ -381,6 +390,7 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
             P.m = (double)m;
             P.floor = -1.0;
             P.idx_bits = bits_for((uint64_t)PL);
+            P.key_vlo = key_vlo_bits(m);
             launch_band(R, P, st);
             MP_LAUNCHED(ctx);
         }
@@ -646,6 +656,7 @@ int mp_eval_diag_block_triangle(mp_context* ctx, double* prof_colmin, int64_t* i
     P.floor = -1.7976931348623157e308;
     const int ib = bits_for((uint64_t)std::max(baserow + T, basecol + T));
     P.idx_bits = ib;
+    P.key_vlo = key_vlo_bits(m);
     launch_band(R, P, st);
     MP_LAUNCHED(ctx);
     block_finalize_kernel<<<grid_for(region), kThreads, 0, st>>>(kex, kid, region, 1, region, ib,

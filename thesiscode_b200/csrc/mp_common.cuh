@@ -38,16 +38,29 @@ __device__ __forceinline__ float unord_f32(unsigned k) {
     return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
 }
 
-// FP64 form, index key: the top (64 - idx_bits) bits order like the distance
-// proxy t = score - m (exact by Sterbenz for score in [m/2, 2m]); the low
-// idx_bits hold (2^idx_bits - 1 - neighbour) so that a max picks the larger
-// score and, among scores whose truncated t agree, the smaller neighbour.
+// FP64 form, index key.  The low idx_bits hold (2^idx_bits - 1 - neighbour),
+// so that among equal high parts a max picks the smaller neighbour.  The high
+// 64 - idx_bits bits order candidates by v = m - score (half the squared
+// distance; exact by Sterbenz for score in [m/2, 2m]), smaller v higher: a
+// region bit (set for v <= 0) and then |v|'s bits taken relative to
+// vlo = 2^(t-64), where the host picks t with 2^t > 2m + 2, so that 64
+// binades need 6 exponent bits instead of 11 and the freed bits keep mantissa
+// (33 mantissa bits at idx_bits = 24: candidates closer than ~1.2e-10 in
+// relative squared distance share a high part).  |v| outside [vlo, 2^t)
+// clamps to the range ends.
 __device__ __forceinline__ unsigned long long idx_key_f64(double score, double m,
                                                           unsigned long long neighbour,
-                                                          int idx_bits) {
+                                                          int idx_bits, long long vlo_bits) {
     const unsigned long long lowmask = (1ull << idx_bits) - 1ull;
-    const unsigned long long hi = ord_f64(score - m) & ~lowmask;
-    return hi | (lowmask - neighbour);
+    const int shift = idx_bits > 5 ? idx_bits - 5 : 0;
+    const long long span = 1ll << 58;  // 64 binades of 2^52 bit patterns
+    const double v = m - score;
+    long long x = __double_as_longlong(fabs(v)) - vlo_bits;
+    x = x < 0 ? 0 : (x > span - 1 ? span - 1 : x);
+    const unsigned long long field =
+        v > 0.0 ? (unsigned long long)(span - 1 - x) >> shift
+                : (1ull << (63 - idx_bits)) | ((unsigned long long)x >> shift);
+    return (field << idx_bits) | (lowmask - neighbour);
 }
 
 // ---------------------------------------------------------------------------

@@ -55,7 +55,7 @@ __device__ __forceinline__ void flush_fp64(const Fp64BandParams& P, int shard, i
     unsigned long long* ke = P.kexact + (int64_t)shard * P.key_stride + slot;
     unsigned long long* ki = P.kidx + (int64_t)shard * P.key_stride + slot;
     atomicMax(ke, ord_f64(score));
-    atomicMax(ki, idx_key_f64(score, P.m, (unsigned long long)neighbour, P.idx_bits));
+    atomicMax(ki, idx_key_f64(score, P.m, (unsigned long long)neighbour, P.idx_bits, P.key_vlo));
 }
 
 // One chunk = R consecutive columns.  Per column the lanes' best cells are

@@ -51,6 +51,7 @@ struct Fp64BandParams {
     double m;
     double floor;  // only scores strictly above it are merged (-1: reference init)
     int idx_bits;
+    long long key_vlo;  // bit pattern of the index key's lower range end (idx_key_f64)
 };
 constexpr int kFp64WarpsPerBlock = 4;
 template <int R>
