@@ -60,3 +60,26 @@ def test_fp64_c3_zero_level_flat_windows(gpu_ctx, oracle, c3z):
     assert flat.sum() == 16 * (m + 1)
     assert np.all(p.dist2[flat] == 2.0 * m + 2.0) and np.all(p.index[flat] == 0)
     assert not np.any(flat[p.index[~flat]] & (p.dist2[~flat] < 2.0 * m + 2.0))
+
+
+@pytest.mark.parametrize("K", [64, 1024])
+def test_fp32_c3_ranges_within_tolerance(gpu_ctx, c3, c3z, K):
+    """FP32 re-anchored vs FP64 on the same diagonals.  Away from the constant
+    stretches (the window and both chosen neighbours farther than m + K from
+    one), the distance error is <= 1e-4 relative wherever the FP64 value is
+    itself accurate.  Windows inside a stretch give the flat result; at zero
+    level both forms follow the reference's flat convention exactly."""
+    for (x, m, segs), zero in ((c3, False), (c3z, True)):
+        PL = x.size - m + 1
+        for lo, hi in _ranges(PL, m):
+            p64 = gpu_ctx.selfjoin(x, m, precision=mp.FP64, diag_lo=lo, diag_hi=hi)
+            p32 = gpu_ctx.selfjoin(x, m, precision=mp.FP32_REANCHOR, reanchor_k=K, diag_lo=lo,
+                                   diag_hi=hi)
+            rep = error_report.compare(x, m, segs, p64, p32, zero, K=K)
+            assert rep["max_rel_far_from_stretches"] <= 1e-4, (zero, lo, hi, rep)
+            assert rep["near_stretch_windows"] <= 0.02 * PL, rep
+            if zero:
+                assert rep["flat_convention_fp32"] and rep["flat_convention_fp64"], rep
+                assert rep["no_window_points_at_flat_fp32"], rep
+            else:
+                assert rep["pseudo_flat_fp32_is_flat_result"], rep

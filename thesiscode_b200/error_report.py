@@ -77,7 +77,18 @@ def pair_distance(x, m: int, i: int, j: int) -> float:
     return float(np.sqrt(max(2.0 * m * (1.0 - rho), 0.0)))
 
 
-def compare(x, m, segs, p64, p32, zero_level: bool, tol: float = 1e-4):
+def stretch_zone(PL: int, m: int, segs, K: int) -> np.ndarray:
+    """Windows that overlap a constant stretch or start within K windows
+    after one: the cells of their diagonals may follow, within one re-anchor
+    interval, cells of windows that straddle the stretch's edges, whose
+    centred dot products are orders of magnitude larger."""
+    zone = np.zeros(PL, dtype=bool)
+    for s, L in segs:
+        zone[max(s - m - K, 0):min(s + L + K, PL)] = True
+    return zone
+
+
+def compare(x, m, segs, p64, p32, zero_level: bool, tol: float = 1e-4, K: int = 1024):
     PL = x.size - m + 1
     none = np.sqrt(2.0 * m + 2.0)  # distance of a window without neighbour
     d64 = np.sqrt(np.abs(p64.dist2))
@@ -110,6 +121,9 @@ def compare(x, m, segs, p64, p32, zero_level: bool, tol: float = 1e-4):
                                      "direct_fp32_pair": e32})
     ok = ~(pseudo | ref_bad)
     rel_ok = rel[ok]
+    zone = stretch_zone(PL, m, segs, K)
+    near = zone | zone[p64.index.clip(0, PL - 1)] | zone[p32.index.clip(0, PL - 1)]
+    far_ok = ok & ~near
     rep = {
         "windows": PL,
         "max_rel_all": float(np.max(rel[~pseudo])),
@@ -121,6 +135,9 @@ def compare(x, m, segs, p64, p32, zero_level: bool, tol: float = 1e-4):
         "reference_inaccurate": int(ref_bad.sum()),
         "fp32_max_rel_vs_direct_on_those": worst_vs_direct,
         "fp32_neighbour_worse_than_fp64": worse_neighbour,
+        "near_stretch_windows": int(near.sum()),
+        "max_rel_far_from_stretches": float(np.max(rel[far_ok])) if far_ok.any() else 0.0,
+        "max_rel_near_stretches": float(np.max(rel[ok & near])) if (ok & near).any() else 0.0,
     }
     if examples:
         rep["worse_neighbour_examples"] = examples
@@ -158,7 +175,7 @@ def run(names, ks, device: int = 0, out=sys.stdout):
                        "fp32_join_ms": join32,
                        "fp64_cells_per_s": cells / (join64 * 1e-3),
                        "fp32_cells_per_s": cells / (join32 * 1e-3)}
-                rep.update(compare(x, m, segs, p64, p32, name == "c3z"))
+                rep.update(compare(x, m, segs, p64, p32, name == "c3z", K=k))
                 print(json.dumps(rep), file=out, flush=True)
 
 
