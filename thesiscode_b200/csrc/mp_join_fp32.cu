@@ -19,7 +19,8 @@
 //             position in the band (lane<<3 | a), so one float min tracks
 //             value and origin at once (2^-15 relative resolution, far
 //             inside the 1e-4 target).  Rows accumulate in registers for R
-//             steps and then in a per-warp shared-memory ring; a column's
+//             steps (columns go in pairs, so one 3-input min takes a cell
+//             of each column) and then in a per-warp shared-memory ring; a column's
 //             warp minimum is one REDUX instruction.  Finished rows/columns
 //             are merged into the profile with a 64-bit atomicMin on
 //             (ordered u, neighbour).
@@ -74,42 +75,92 @@ __device__ __forceinline__ void flush_row(const Fp32TileParams& P, float v, int6
 // no divergent branch between steps (consecutive steps can overlap).  Row
 // partials live in a 2R-entry circular register array; OFF (0 or R) is the
 // chunk's rotation, so no register ever moves between chunks.
+// Slow chunks (near the end of a band) mask cells past the diagonal's end:
+// cell (column jr + b, diagonal g0 + d) exists iff d < ghi_rel and
+// jr + b < min(lim0 - d, ncols).
 template <int R, bool FAST, int OFF>
 __device__ __forceinline__ void chunk_fp32(const char* rbase, const char* cbuf,
                                            RowRec (&win)[R / 2], float2 (&nc2)[R / 2],
                                            float (&acc)[2 * R], const unsigned (&tag)[R],
-                                           const int (&limr)[R], int jr, int lane, int& colkey) {
+                                           int lim0, int ncols, int ghi_rel, int jr, int lane,
+                                           int& colkey) {
     constexpr int H = R / 2;
+    static_assert(R % 2 == 0, "columns are processed in pairs");
+    // Columns go in pairs (b, b + 1): row slot s = b + d takes cell d of
+    // column b and cell d - 1 of column b + 1, so one 3-input min per slot
+    // serves both columns (9 row-min instructions per 2R cells, not 2R).
 #pragma unroll
-    for (int b = 0; b < R; ++b) {
+    for (int b = 0; b < R; b += 2) {
+        float kb[R];  // column b's tagged cells, by diagonal
         {
-            // record tbase + b + H - 1; tbase % 8 == 0, so its slot % 8 == H - 1
-            const char* p = rbase + rec_step<H - 1>(b);
-            win[(b + H - 1) % H].dfdg = *reinterpret_cast<const float4*>(p);
-            win[(b + H - 1) % H].nn1 = *reinterpret_cast<const float4*>(p + 16);
-        }
-        const float4 cv = *reinterpret_cast<const float4*>(cbuf + 32 * b);
-        const float2 cnn = *reinterpret_cast<const float2*>(cbuf + 32 * b + 16);
-        float cmin = kInf;
-#pragma unroll
-        for (int a = 0; a < H; ++a) {
-            const RowRec& rv = win[(b + a) % H];
-            const float2 nn2 = __fmul2_rn(cnn, lo2(rv.nn1));
-            const float2 u2 = __ffma2_rn(nc2[a], nn2, hi2(rv.nn1));
-            nc2[a] = __ffma2_rn(lo2(cv), hi2(rv.dfdg), nc2[a]);
-            nc2[a] = __ffma2_rn(lo2(rv.dfdg), hi2(cv), nc2[a]);
-            float k0 = tag_key(u2.x, tag[a]);
-            float k1 = tag_key(u2.y, tag[a + H]);
-            if (!FAST) {
-                if (jr + b >= limr[a]) k0 = kInf;
-                if (jr + b >= limr[a + H]) k1 = kInf;
+            {
+                // record tbase + b + H - 1; tbase % 8 == 0, so its slot % 8 == H - 1
+                const char* p = rbase + rec_step<H - 1>(b);
+                win[(b + H - 1) % H].dfdg = *reinterpret_cast<const float4*>(p);
+                win[(b + H - 1) % H].nn1 = *reinterpret_cast<const float4*>(p + 16);
             }
-            acc[(b + a + OFF) % (2 * R)] = fminf(acc[(b + a + OFF) % (2 * R)], k0);
-            acc[(b + a + H + OFF) % (2 * R)] = fminf(acc[(b + a + H + OFF) % (2 * R)], k1);
-            cmin = fmin3(cmin, k0, k1);
+            const float4 cv = *reinterpret_cast<const float4*>(cbuf + 32 * b);
+            const float2 cnn = *reinterpret_cast<const float2*>(cbuf + 32 * b + 16);
+            float cmin = kInf;
+#pragma unroll
+            for (int a = 0; a < H; ++a) {
+                const RowRec& rv = win[(b + a) % H];
+                const float2 nn2 = __fmul2_rn(cnn, lo2(rv.nn1));
+                const float2 u2 = __ffma2_rn(nc2[a], nn2, hi2(rv.nn1));
+                nc2[a] = __ffma2_rn(lo2(cv), hi2(rv.dfdg), nc2[a]);
+                nc2[a] = __ffma2_rn(lo2(rv.dfdg), hi2(cv), nc2[a]);
+                kb[a] = tag_key(u2.x, tag[a]);
+                kb[a + H] = tag_key(u2.y, tag[a + H]);
+                if (!FAST) {
+                    const int l0 = a < ghi_rel ? min(lim0 - a, ncols) : 0;
+                    const int l1 = a + H < ghi_rel ? min(lim0 - a - H, ncols) : 0;
+                    if (jr + b >= l0) kb[a] = kInf;
+                    if (jr + b >= l1) kb[a + H] = kInf;
+                }
+                cmin = fmin3(cmin, kb[a], kb[a + H]);
+            }
+            acc[(b + OFF) % (2 * R)] = fminf(acc[(b + OFF) % (2 * R)], kb[0]);
+            const int kmin = __reduce_min_sync(kFullMask, __float_as_int(cmin));
+            colkey = (lane == b + OFF) ? kmin : colkey;
         }
-        const int kmin = __reduce_min_sync(kFullMask, __float_as_int(cmin));
-        colkey = (lane == b + OFF) ? kmin : colkey;
+        {
+            const int c = b + 1;
+            {
+                const char* p = rbase + rec_step<H - 1>(c);
+                win[(c + H - 1) % H].dfdg = *reinterpret_cast<const float4*>(p);
+                win[(c + H - 1) % H].nn1 = *reinterpret_cast<const float4*>(p + 16);
+            }
+            const float4 cv = *reinterpret_cast<const float4*>(cbuf + 32 * c);
+            const float2 cnn = *reinterpret_cast<const float2*>(cbuf + 32 * c + 16);
+            float cmin = kInf;
+#pragma unroll
+            for (int a = 0; a < H; ++a) {
+                const RowRec& rv = win[(c + a) % H];
+                const float2 nn2 = __fmul2_rn(cnn, lo2(rv.nn1));
+                const float2 u2 = __ffma2_rn(nc2[a], nn2, hi2(rv.nn1));
+                nc2[a] = __ffma2_rn(lo2(cv), hi2(rv.dfdg), nc2[a]);
+                nc2[a] = __ffma2_rn(lo2(rv.dfdg), hi2(cv), nc2[a]);
+                float k0 = tag_key(u2.x, tag[a]);
+                float k1 = tag_key(u2.y, tag[a + H]);
+                if (!FAST) {
+                    const int l0 = a < ghi_rel ? min(lim0 - a, ncols) : 0;
+                    const int l1 = a + H < ghi_rel ? min(lim0 - a - H, ncols) : 0;
+                    if (jr + c >= l0) k0 = kInf;
+                    if (jr + c >= l1) k1 = kInf;
+                }
+                // slot c + a: cell a of column c and cell a + 1 of column b
+                acc[(c + a + OFF) % (2 * R)] = fmin3(acc[(c + a + OFF) % (2 * R)], k0, kb[a + 1]);
+                // slot c + a + H: cell a + H of column c and cell a + H + 1 of column b
+                if (a + H + 1 < R)
+                    acc[(c + a + H + OFF) % (2 * R)] =
+                        fmin3(acc[(c + a + H + OFF) % (2 * R)], k1, kb[a + H + 1]);
+                else
+                    acc[(c + a + H + OFF) % (2 * R)] = fminf(acc[(c + a + H + OFF) % (2 * R)], k1);
+                cmin = fmin3(cmin, k0, k1);
+            }
+            const int kmin = __reduce_min_sync(kFullMask, __float_as_int(cmin));
+            colkey = (lane == c + OFF) ? kmin : colkey;
+        }
     }
 }
 
@@ -126,17 +177,17 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
     if (j0 >= j1) return;
     const float ulim = (float)(1.0 + 1.0 / (double)P.m);
 
-    // cell (column j, diagonal g) is evaluated iff j - j0 < limr
-    int limr[R];
-    int minlim = INT32_MAX;
+    // cell (column j, diagonal g0 + d) is evaluated iff d < ghi_rel and
+    // j - j0 < min(lim0 - d, ncols); every cell of a chunk ending at or
+    // before minlim exists
+    const int ncols = (int)(j1 - j0);
+    const int lim0 = (int)min(P.PL - g0 - j0, (int64_t)ncols + R);
+    const int ghi_rel = (int)max(min(P.g_hi - g0, (int64_t)R), (int64_t)0);
+    const int minlim = ghi_rel < R ? 0 : min(lim0 - (R - 1), ncols);
+    // tag of cell d: lane << 3 | d
     unsigned tag[R];
 #pragma unroll
-    for (int a = 0; a < R; ++a) {
-        const int64_t g = g0 + a;
-        limr[a] = (g < P.g_hi) ? (int)(min(P.PL - g, j1) - j0) : 0;
-        minlim = min(minlim, limr[a]);
-        tag[a] = ((unsigned)lane << 3) | (unsigned)a;
-    }
+    for (int a = 0; a < R; ++a) tag[a] = ((unsigned)lane << 3) | (unsigned)a;
 
     // ---- FP64 re-anchor: cov(j0, j0+g) for the lane's R diagonals ----------
     double q[R];
@@ -210,7 +261,6 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
     int cb = 0;                              // column buffer of the current pair
     int rslot = rec_slot(lane * R + H - 1);  // record slot of jr + lane*R + H - 1
     int kslot = lane;                        // (jr / R + lane) % RK_CHUNKS
-    const int ncols = (int)(j1 - j0);
     int jr = 0;
     for (; jr < ncols; jr += 2 * R) {
         // prefetch what the next pair appends: 2R row records and 2R column records
@@ -227,16 +277,16 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
             const bool fast = __all_sync(kFullMask, jh + R <= minlim);
             if (half == 0) {
                 if (fast)
-                    chunk_fp32<R, true, 0>(rbase, cbuf, win, nc2, acc, tag, limr, jh, lane, colkey);
+                    chunk_fp32<R, true, 0>(rbase, cbuf, win, nc2, acc, tag, lim0, ncols, ghi_rel, jh, lane, colkey);
                 else
-                    chunk_fp32<R, false, 0>(rbase, cbuf, win, nc2, acc, tag, limr, jh, lane, colkey);
+                    chunk_fp32<R, false, 0>(rbase, cbuf, win, nc2, acc, tag, lim0, ncols, ghi_rel, jh, lane, colkey);
             } else {
                 if (fast)
-                    chunk_fp32<R, true, R>(rbase, cbuf + 32 * R, win, nc2, acc, tag, limr, jh, lane,
-                                           colkey);
+                    chunk_fp32<R, true, R>(rbase, cbuf + 32 * R, win, nc2, acc, tag, lim0,
+                                           ncols, ghi_rel, jh, lane, colkey);
                 else
-                    chunk_fp32<R, false, R>(rbase, cbuf + 32 * R, win, nc2, acc, tag, limr, jh,
-                                            lane, colkey);
+                    chunk_fp32<R, false, R>(rbase, cbuf + 32 * R, win, nc2, acc, tag,
+                                            lim0, ncols, ghi_rel, jh, lane, colkey);
             }
             // this chunk's lower half (rows jh + g0 + [0, R)) is final for the lane
             const int ks = (kslot + half) >= RK_CHUNKS ? kslot + half - RK_CHUNKS : kslot + half;
