@@ -36,11 +36,16 @@ namespace mpgpu {
 
 namespace {
 
+// A row record in memory (global and the shared-memory ring): 32 bytes.
 struct RowRec {
     float4 dfdg;  // (df[j], df[j+H], dg[j], dg[j+H])
-    float4 nn1;   // (nn[j], nn[j+H], 1, 1): the constant pair rides along with the
-                  // record so the fused u = 1 + nc*nn never needs a
-                  // rematerialised immediate register pair
+    float4 nn1;   // (nn[j], nn[j+H], 1, 1)
+};
+// The part of a row record a lane keeps in registers (the constant pair stays
+// behind: one shared (1, 1) operand serves every fused distance).
+struct RowWin {
+    float4 dfdg;
+    float2 nn;
 };
 __device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
 __device__ __forceinline__ float2 hi2(const float4& v) { return make_float2(v.z, v.w); }
@@ -80,12 +85,13 @@ __device__ __forceinline__ void flush_row(const Fp32TileParams& P, float v, int6
 // jr + b < min(lim0 - d, ncols).
 template <int R, bool FAST, int OFF>
 __device__ __forceinline__ void chunk_fp32(const char* rbase, const char* cbuf,
-                                           RowRec (&win)[R / 2], float2 (&nc2)[R / 2],
+                                           RowWin (&win)[R / 2], float2 (&nc2)[R / 2],
                                            float (&acc)[2 * R], const unsigned (&tag)[R],
                                            int lim0, int ncols, int ghi_rel, int jr, int lane,
                                            int& colkey) {
     constexpr int H = R / 2;
     static_assert(R % 2 == 0, "columns are processed in pairs");
+    const float2 one2 = make_float2(1.f, 1.f);
     // Columns go in pairs (b, b + 1): row slot s = b + d takes cell d of
     // column b and cell d - 1 of column b + 1, so one 3-input min per slot
     // serves both columns (9 row-min instructions per 2R cells, not 2R).
@@ -97,16 +103,16 @@ __device__ __forceinline__ void chunk_fp32(const char* rbase, const char* cbuf,
                 // record tbase + b + H - 1; tbase % 8 == 0, so its slot % 8 == H - 1
                 const char* p = rbase + rec_step<H - 1>(b);
                 win[(b + H - 1) % H].dfdg = *reinterpret_cast<const float4*>(p);
-                win[(b + H - 1) % H].nn1 = *reinterpret_cast<const float4*>(p + 16);
+                win[(b + H - 1) % H].nn = *reinterpret_cast<const float2*>(p + 16);
             }
             const float4 cv = *reinterpret_cast<const float4*>(cbuf + 32 * b);
             const float2 cnn = *reinterpret_cast<const float2*>(cbuf + 32 * b + 16);
-            float cmin = kInf;
+            float cmin;
 #pragma unroll
             for (int a = 0; a < H; ++a) {
-                const RowRec& rv = win[(b + a) % H];
-                const float2 nn2 = __fmul2_rn(cnn, lo2(rv.nn1));
-                const float2 u2 = __ffma2_rn(nc2[a], nn2, hi2(rv.nn1));
+                const RowWin& rv = win[(b + a) % H];
+                const float2 nn2 = __fmul2_rn(cnn, rv.nn);
+                const float2 u2 = __ffma2_rn(nc2[a], nn2, one2);
                 nc2[a] = __ffma2_rn(lo2(cv), hi2(rv.dfdg), nc2[a]);
                 nc2[a] = __ffma2_rn(lo2(rv.dfdg), hi2(cv), nc2[a]);
                 kb[a] = tag_key(u2.x, tag[a]);
@@ -117,7 +123,7 @@ __device__ __forceinline__ void chunk_fp32(const char* rbase, const char* cbuf,
                     if (jr + b >= l0) kb[a] = kInf;
                     if (jr + b >= l1) kb[a + H] = kInf;
                 }
-                cmin = fmin3(cmin, kb[a], kb[a + H]);
+                cmin = a == 0 ? fminf(kb[a], kb[a + H]) : fmin3(cmin, kb[a], kb[a + H]);
             }
             acc[(b + OFF) % (2 * R)] = fminf(acc[(b + OFF) % (2 * R)], kb[0]);
             const int kmin = __reduce_min_sync(kFullMask, __float_as_int(cmin));
@@ -128,16 +134,16 @@ __device__ __forceinline__ void chunk_fp32(const char* rbase, const char* cbuf,
             {
                 const char* p = rbase + rec_step<H - 1>(c);
                 win[(c + H - 1) % H].dfdg = *reinterpret_cast<const float4*>(p);
-                win[(c + H - 1) % H].nn1 = *reinterpret_cast<const float4*>(p + 16);
+                win[(c + H - 1) % H].nn = *reinterpret_cast<const float2*>(p + 16);
             }
             const float4 cv = *reinterpret_cast<const float4*>(cbuf + 32 * c);
             const float2 cnn = *reinterpret_cast<const float2*>(cbuf + 32 * c + 16);
-            float cmin = kInf;
+            float cmin;
 #pragma unroll
             for (int a = 0; a < H; ++a) {
-                const RowRec& rv = win[(c + a) % H];
-                const float2 nn2 = __fmul2_rn(cnn, lo2(rv.nn1));
-                const float2 u2 = __ffma2_rn(nc2[a], nn2, hi2(rv.nn1));
+                const RowWin& rv = win[(c + a) % H];
+                const float2 nn2 = __fmul2_rn(cnn, rv.nn);
+                const float2 u2 = __ffma2_rn(nc2[a], nn2, one2);
                 nc2[a] = __ffma2_rn(lo2(cv), hi2(rv.dfdg), nc2[a]);
                 nc2[a] = __ffma2_rn(lo2(rv.dfdg), hi2(cv), nc2[a]);
                 float k0 = tag_key(u2.x, tag[a]);
@@ -150,13 +156,17 @@ __device__ __forceinline__ void chunk_fp32(const char* rbase, const char* cbuf,
                 }
                 // slot c + a: cell a of column c and cell a + 1 of column b
                 acc[(c + a + OFF) % (2 * R)] = fmin3(acc[(c + a + OFF) % (2 * R)], k0, kb[a + 1]);
-                // slot c + a + H: cell a + H of column c and cell a + H + 1 of column b
-                if (a + H + 1 < R)
+                // slot c + a + H: cell a + H of column c and cell a + H + 1 of column
+                // b.  Slots b + R - 1 and b + R begin new rows here (these are their
+                // first cells), so they are assigned and no slot needs a reset.
+                if (a == H - 1)
+                    acc[(c + a + H + OFF) % (2 * R)] = k1;
+                else if (a == H - 2)
+                    acc[(c + a + H + OFF) % (2 * R)] = fminf(k1, kb[a + H + 1]);
+                else
                     acc[(c + a + H + OFF) % (2 * R)] =
                         fmin3(acc[(c + a + H + OFF) % (2 * R)], k1, kb[a + H + 1]);
-                else
-                    acc[(c + a + H + OFF) % (2 * R)] = fminf(acc[(c + a + H + OFF) % (2 * R)], k1);
-                cmin = fmin3(cmin, k0, k1);
+                cmin = a == 0 ? fminf(k0, k1) : fmin3(cmin, k0, k1);
             }
             const int kmin = __reduce_min_sync(kFullMask, __float_as_int(cmin));
             colkey = (lane == c + OFF) ? kmin : colkey;
@@ -245,12 +255,12 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
         reinterpret_cast<const RowRec*>(P.colrec) + j0);
     *reinterpret_cast<uint4*>(cring + 16 * lane) = __ldg(csrc + lane);
     __syncwarp();
-    RowRec win[H];
+    RowWin win[H];
 #pragma unroll
     for (int k = 0; k < H - 1; ++k) {
         const char* p = rring + rec_off(rec_slot(lane * R + k));
         win[k].dfdg = *reinterpret_cast<const float4*>(p);
-        win[k].nn1 = *reinterpret_cast<const float4*>(p + 16);
+        win[k].nn = *reinterpret_cast<const float2*>(p + 16);
     }
 
     // Row partials leave the registers through a ring of RK slots in shared
@@ -300,8 +310,6 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
                 t.w = fminf(t.w, acc[(4 * v + 3 + half * R) % (2 * R)]);
                 rv4[v] = t;
             }
-#pragma unroll
-            for (int k = 0; k < R; ++k) acc[(k + half * R) % (2 * R)] = kInf;
         }
         kslot += 2;
         if (kslot >= RK_CHUNKS) kslot -= RK_CHUNKS;
