@@ -330,11 +330,11 @@ def run_ours(args, world):
         except Exception:
             peaks[name] = None
     peak32 = max(v for v in (peaks["f32_ffma"], peaks["f32x2_ffma2"]) if v)
-    traffic = read_ncu_traffic("fp32_tile_kernel_c2")
+    traffic = read_ncu_traffic("fp32_join_kernel_c2")
     roofline = {
         "bound": "fp32-fma-pipe (CUDA cores; no tensor-core or HBM bound)",
         "achieved": achieved, "peak": peak32, "unit": "TFLOP/s", "frac": achieved / peak32,
-        "traffic": traffic, "kernel": "fp32_tile_kernel<8>",
+        "traffic": traffic, "kernel": "fp32_join_kernel<8>",
         "algorithmic_flops_per_launch": FLOP_PER_CELL * cells_mine,
         "kernel_ms": join_avg_ms,
         "peak_source": "measured in this run: independent-FMA-chain kernel (mp_measure_fma_peak), "

@@ -73,3 +73,26 @@ def test_run_algorithm_through_registry(tmp_path, golden_ascii):
     got = np.loadtxt(out)
     assert np.array_equal(got[:, 1].astype(np.int64), golden_ascii["idx_m16"])
     assert mp.run_algorithm("no_such_variant", str(inp), str(out), 16) == mp.MP_ERR_INVALID_ARG
+
+
+def test_cli_outputs_pass_the_validation_tool(tmp_path, golden_ascii):
+    """The reference's validation workflow on the drop-in CLI's files: the FP64
+    variant's profile coincides with the reference's profile; the FP32
+    variant's indices agree up to neighbours whose distances tie within 1e-4."""
+    from thesiscode_b200 import validate
+    x = golden_ascii["series"]
+    inp = tmp_path / "test.ascii"
+    _write_ascii(inp, x)
+    ref = tmp_path / "ref.ascii"
+    validate.write_profile_ascii(str(ref), golden_ascii["d2_m64"], golden_ascii["idx_m64"])
+    outs = {}
+    for algo in ("gpu_vert_blocked_fp64", "gpu_vert_blocked_fp32k"):
+        outs[algo] = tmp_path / f"{algo}.matprof.ascii"
+        r = subprocess.run([mp.CLI_PATH, algo, "64", "16", str(inp),
+                            "--output-file", str(outs[algo])], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+    assert validate.main(["compare", str(ref), str(outs["gpu_vert_blocked_fp64"]),
+                          "--silent"]) == 0
+    assert validate.main(["compare", str(outs["gpu_vert_blocked_fp64"]),
+                          str(outs["gpu_vert_blocked_fp32k"]), "--silent", "--series", str(inp),
+                          "--window", "64", "--rel-tol", "1e-4"]) == 0
