@@ -42,7 +42,8 @@ typedef enum {
      * separately rounded per-cell steps as the reference's AVX2 kernel.
      * Profile values are bit-identical to the reference compiled with IEEE
      * semantics; indices agree except between candidates whose squared
-     * distances tie to within 2^-29 relative (n <= 2^23). */
+     * distances tie to within ~1.2e-10 relative (n <= 2^24), where the
+     * smaller neighbour index is kept. */
     MP_PREC_FP64 = 0,
     /* FP32 covariance recurrence re-anchored every reanchor_k steps by an FP64
      * dot product; window means/norms in FP64 (Welford). */
@@ -210,6 +211,27 @@ int mp_server_destroy(mp_server* s);
 int mp_selfjoin_fp32_noalloc(const double* A_dev, int64_t n, int64_t m, int64_t excl,
                              int64_t reanchor_k, double* dist2_dev, int64_t* idx_dev,
                              void* stream, char* err, size_t err_len);
+
+/*
+ * PreSCRIMP, the anytime front end of SCRIMP++ (replaces the PreSCRIMP phase
+ * of ScrimpppOrig::compute_matrix_profile, scrimppp/src/ScrimpppOrig.cpp:
+ * 130-266).  Query windows i = 0, s, 2s, ... with s = floor(stride * m) get
+ * their whole distance profile (windows j with |j - i| < m/4 excluded, as in
+ * the reference); every evaluated cell lowers both windows' entries; then each
+ * query's best diagonal is walked s - 1 cells forward and backward.  The
+ * result is an approximate profile (an upper bound of the exact one) in
+ * squared distances, with the reference's initial values (+inf, index 0) for
+ * windows no cell reached.  The reference convolves with FFTW; the GPU forms
+ * each query cell as a direct FP64 dot product, so values agree with the
+ * reference to rounding, not bit for bit, and every update is a min-merge
+ * (independent of the reference's shuffled query order).
+ *   A            n doubles, host or device memory.
+ *   stride       the reference's --prescrimp-stride (s = floor(stride * m) >= 1).
+ *   dist2_out    PL doubles, idx_out PL int64 (host or device, same space).
+ * Synchronous on stream.
+ */
+int mp_prescrimp(mp_context* ctx, const double* A, int64_t n, int64_t m, double stride,
+                 double* dist2_out, int64_t* idx_out, void* stream);
 
 /* FMA throughput of this device's CUDA-core pipes in FLOP/s (2 per FMA),
  * measured with independent FMA chains: which = 0 FP32 (FFMA), 1 FP32 (f32x2

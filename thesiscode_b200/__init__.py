@@ -48,7 +48,7 @@ EXPORTED_SYMBOLS = (
     "mp_batch_create", "mp_batch_destroy", "mp_batch_cells", "mp_batch_tiles",
     "mp_batch_launch_count", "mp_batch_upload", "mp_batch_launch", "mp_batch_download",
     "mp_batch_run", "mp_server_create", "mp_server_submit", "mp_server_poll", "mp_server_collect",
-    "mp_server_stats", "mp_server_destroy", "mp_selfjoin_fp32_noalloc",
+    "mp_server_stats", "mp_server_destroy", "mp_selfjoin_fp32_noalloc", "mp_prescrimp",
 )
 
 
@@ -86,6 +86,7 @@ def load_library() -> ctypes.CDLL:
                                               _P, _P, _P, _P, _i64, _i64, _P]
     L.mp_window_stats.argtypes = [_P, _P, _i64, _i64, _P, _P, _P]
     L.mp_first_qt.argtypes = [_P, _P, _i64, _i64, _i64, _i64, _P, _P]
+    L.mp_prescrimp.argtypes = [_P, _P, _i64, _i64, ctypes.c_double, _P, _P, _P]
     L.mp_last_launch_count.argtypes = [_P]
     L.mp_last_launch_count.restype = _i64
     L.mp_set_phase_timing.argtypes = [_P, ctypes.c_int]
@@ -240,6 +241,26 @@ class Context:
         rc = self._L.mp_selfjoin(self._h, _ptr(A), n, m, excl, precision, reanchor_k, blocklen,
                                  diag_lo, diag_hi, _ptr(d2), _ptr(ix), stream)
         self._check(rc)
+        return Profile(d2, ix)
+
+    def prescrimp(self, A, m: int, stride: float, out=None, stream=None) -> Profile:
+        """PreSCRIMP approximate profile (the SCRIMP++ front end): query windows
+        every floor(stride * m), their whole distance profiles and the walks along
+        each query's best diagonal.  Squared distances; +inf / index 0 where no
+        evaluated cell reached a window."""
+        if isinstance(A, np.ndarray):
+            A = np.ascontiguousarray(A, dtype=np.float64)
+            n = A.size
+        else:
+            n = A.numel()
+        PL = n - m + 1
+        if out is None:
+            d2 = np.empty(max(PL, 0), dtype=np.float64)
+            ix = np.empty(max(PL, 0), dtype=np.int64)
+        else:
+            d2, ix = out
+        self._check(self._L.mp_prescrimp(self._h, _ptr(A), n, m, float(stride), _ptr(d2),
+                                         _ptr(ix), stream))
         return Profile(d2, ix)
 
     def window_stats(self, A, m: int):

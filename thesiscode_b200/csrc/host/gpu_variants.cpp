@@ -88,6 +88,9 @@ public:
         store_profile(params, d2, idx);
     }
 
+protected:
+    mp_context* context() const { return ctx_; }
+
 private:
     int precision_;
     mp_context* ctx_ = nullptr;
@@ -102,7 +105,44 @@ public:
     GpuVertBlockedFp32K() : GpuVertBlocked(MP_PREC_FP32_REANCHOR) {}
 };
 
+// SCRIMP++ (ScrimpppOrig::compute_matrix_profile, scrimppp/src/ScrimpppOrig.cpp:
+// 37-395): the PreSCRIMP approximate profile goes to "<output>_prescrimp"
+// (always ASCII, as the reference writes it, :268-279), then the exact
+// profile of all diagonals to <output>.  The exact phase is the FP64 form:
+// the same values as scrimp_vert_blocked; the reference's own SCRIMP phase
+// forms distances with sqrt-variance arithmetic (:300-330) and agrees with
+// them to rounding.
+class GpuScrimppp : public GpuVertBlocked {
+public:
+    GpuScrimppp() : GpuVertBlocked(MP_PREC_FP64) {}
+    void compute_matrix_profile(const Scrimppp_params& params) override {
+        initialize(params);
+        const std::vector<double> A = fetch_series(params);
+        const int64_t n = (int64_t)A.size(), m = params.query_window_len;
+        if (m < 2 || n < m)
+            throw std::runtime_error(
+                "ERROR: Time series is shorter than the window length, can not proceed");
+        const int64_t PL = n - m + 1;
+        std::vector<double> d2(PL);
+        std::vector<int64_t> idx(PL);
+        const auto t0 = std::chrono::steady_clock::now();
+        const int rc = mp_prescrimp(context(), A.data(), n, m, (double)params.prescrimp_stride,
+                                    d2.data(), idx.data(), nullptr);
+        if (rc != MP_OK)
+            throw std::runtime_error(std::string("mp_prescrimp: ") + mp_status_string(rc) + ": " +
+                                     mp_last_error(context()));
+        std::clog << "Time for PreSCRIMP: " << std::setprecision(17)
+                  << std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count()
+                  << std::endl;
+        if (params.output_filename.empty())
+            throw std::runtime_error("Empty output file name specified!");
+        io::write_profile_ascii(params.output_filename + "_prescrimp", d2.data(), idx.data(), PL);
+        GpuVertBlocked::compute_matrix_profile(params);
+    }
+};
+
 FactoryRegistration<GpuVertBlockedFp64> reg_fp64("gpu_vert_blocked_fp64");
+FactoryRegistration<GpuScrimppp> reg_scrimppp("gpu_scrimppp");
 FactoryRegistration<GpuVertBlockedFp32K> reg_fp32("gpu_vert_blocked_fp32k");
 
 }  // namespace

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -514,6 +515,89 @@ int mp_window_stats(mp_context* ctx, const double* A, int64_t n, int64_t m, doub
     MP_LAUNCHED(ctx);
     MP_CUDA(ctx, cudaMemcpyAsync(muS_out, mu, 8 * PL, cudaMemcpyDefault, st));
     MP_CUDA(ctx, cudaMemcpyAsync(sInv_out, si, 8 * PL, cudaMemcpyDefault, st));
+    MP_CUDA(ctx, cudaStreamSynchronize(st));
+    return MP_OK;
+}
+
+int mp_prescrimp(mp_context* ctx, const double* A, int64_t n, int64_t m, double stride,
+                 double* dist2_out, int64_t* idx_out, void* stream) {
+    if (!ctx) return MP_ERR_INVALID_ARG;
+    if (!A || !dist2_out || !idx_out) return fail(ctx, MP_ERR_INVALID_ARG, "null buffer");
+    if (m < 2) return fail(ctx, MP_ERR_INVALID_ARG, "window length m=%lld < 2", (long long)m);
+    if (n < m)
+        return fail(ctx, MP_ERR_INVALID_ARG,
+                    "time series is shorter than the window length (n=%lld, m=%lld)",
+                    (long long)n, (long long)m);
+    const int64_t PL = n - m + 1;
+    if (PL >= (1ll << 31))
+        return fail(ctx, MP_ERR_NOT_SUPPORTED, "profile length %lld exceeds 2^31-1", (long long)PL);
+    // ScrimpppOrig.cpp:49: stepSize = floor(prescrimp_stride * windowSize)
+    const double stepf = std::floor(stride * (double)m);
+    if (!(stepf >= 1.0) || stepf > (double)INT32_MAX)
+        return fail(ctx, MP_ERR_INVALID_ARG, "PreSCRIMP step floor(%g * %lld) must be >= 1",
+                    stride, (long long)m);
+    MP_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    ctx->launches = 0;
+    const int64_t step = (int64_t)stepf;
+    const int64_t Q = (PL + step - 1) / step;
+    const bool o_dev = on_device(dist2_out);
+    if (on_device(idx_out) != o_dev)
+        return fail(ctx, MP_ERR_INVALID_ARG, "dist2_out and idx_out live in different memory spaces");
+    size_t bytes = align_up(8 * (size_t)n) * 3 + align_up(8 * (size_t)PL) * 4 +
+                   align_up(8 * (size_t)Q) * 2 + 4096;
+    if (!o_dev) bytes += align_up(8 * (size_t)PL) * 2;
+    int rc = reserve(ctx, bytes);
+    if (rc) return rc;
+    Carve cv{(char*)ctx->arena};
+    double* Ad = cv.take<double>(n);
+    double* cs = cv.take<double>(n);
+    double* cs2 = cv.take<double>(n);
+    double* mean = cv.take<double>(PL);
+    double* sigma = cv.take<double>(PL);
+    unsigned long long* kex = cv.take<unsigned long long>(PL);
+    unsigned long long* kix = cv.take<unsigned long long>(PL);
+    unsigned long long* rex = cv.take<unsigned long long>(Q);
+    unsigned long long* rix = cv.take<unsigned long long>(Q);
+    double* d2 = o_dev ? dist2_out : cv.take<double>(PL);
+    int64_t* ix = o_dev ? idx_out : cv.take<int64_t>(PL);
+    MP_CUDA(ctx, cudaMemcpyAsync(Ad, A, 8 * n, cudaMemcpyDefault, st));
+    ref_prefix_kernel<<<1, 1, 0, st>>>(Ad, n, cs, cs2);
+    MP_LAUNCHED(ctx);
+    orig_stats_kernel<<<grid_for(PL), kThreads, 0, st>>>(cs, cs2, PL, m, mean, sigma);
+    MP_LAUNCHED(ctx);
+    prescrimp_keys_init_kernel<<<grid_for(PL), kThreads, 0, st>>>(kex, PL);
+    MP_LAUNCHED(ctx);
+    prescrimp_keys_init_kernel<<<grid_for(PL), kThreads, 0, st>>>(kix, PL);
+    MP_LAUNCHED(ctx);
+    prescrimp_keys_init_kernel<<<grid_for(Q), kThreads, 0, st>>>(rex, Q);
+    MP_LAUNCHED(ctx);
+    prescrimp_keys_init_kernel<<<grid_for(Q), kThreads, 0, st>>>(rix, Q);
+    MP_LAUNCHED(ctx);
+    PreScrimpParams P{};
+    P.A = Ad;
+    P.mean = mean;
+    P.sigma = sigma;
+    P.n = n;
+    P.m = m;
+    P.PL = PL;
+    P.excl = m / 4;  // ScrimpppOrig.cpp:73
+    P.step = step;
+    P.Q = Q;
+    P.kex = kex;
+    P.kix = kix;
+    P.rex = rex;
+    P.rix = rix;
+    P.idx_bits = bits_for((uint64_t)PL);
+    launch_prescrimp(P, st);  // two kernels
+    ++ctx->launches;
+    MP_LAUNCHED(ctx);
+    prescrimp_finalize_kernel<<<grid_for(PL), kThreads, 0, st>>>(kex, kix, PL, P.idx_bits, d2, ix);
+    MP_LAUNCHED(ctx);
+    if (!o_dev) {
+        MP_CUDA(ctx, cudaMemcpyAsync(dist2_out, d2, 8 * PL, cudaMemcpyDeviceToHost, st));
+        MP_CUDA(ctx, cudaMemcpyAsync(idx_out, ix, 8 * PL, cudaMemcpyDeviceToHost, st));
+    }
     MP_CUDA(ctx, cudaStreamSynchronize(st));
     return MP_OK;
 }

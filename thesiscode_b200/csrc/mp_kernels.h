@@ -84,6 +84,29 @@ void configure_fp32_join();
 void fp32_tile_plan(int64_t PL, int64_t g_lo, int64_t g_hi, int64_t K, int R, int64_t& nbands,
                     int64_t& seg_per_pair, int64_t& ntiles);
 
+// ---- PreSCRIMP (mp_prescrimp.cu) -------------------------------------------------
+struct PreScrimpParams {
+    const double* A;      // series, n samples
+    const double* mean;   // window means (reference order)
+    const double* sigma;  // window standard deviations (reference order)
+    int64_t n, m, PL, excl;
+    int64_t step;         // floor(stride * m): query i_t = t * step
+    int64_t Q;            // number of queries
+    unsigned long long* kex;  // [PL] ordered distance, min-merged
+    unsigned long long* kix;  // [PL] ordered distance (high bits) | neighbour, min-merged
+    unsigned long long* rex;  // [Q] a query's own best (distance)
+    unsigned long long* rix;  // [Q] ... (neighbour)
+    int idx_bits;
+};
+__global__ void orig_stats_kernel(const double* cs, const double* cs2, int64_t PL, int64_t m,
+                                  double* mean, double* sigma);
+__global__ void prescrimp_keys_init_kernel(unsigned long long* a, int64_t count);
+__global__ void prescrimp_finalize_kernel(const unsigned long long* kex,
+                                          const unsigned long long* kix, int64_t PL, int idx_bits,
+                                          double* d2, int64_t* idx);
+// Query rows then diagonal walks (2 launches).
+void launch_prescrimp(const PreScrimpParams& P, cudaStream_t s);
+
 // ---- finalisation (mp_finalize.cu) -------------------------------------------
 __global__ void init_keys_kernel(unsigned long long* k, int64_t count, unsigned long long v);
 __global__ void finalize_fp64_kernel(const unsigned long long* kexact, const unsigned long long* kidx,
