@@ -284,31 +284,66 @@ def run_ours(args, world):
     value64 = cells_total * fsteps / (tot64 * 1e-3)
     fp64_d2 = d2.cpu().numpy().copy()
 
-    # -- end to end through the C ABI with pinned host buffers -------------------
-    e2e = None
-    lat = None
-    if world == 1:
-        xh = torch.from_numpy(x).pin_memory()
-        oh = (torch.empty(PL, dtype=torch.float64).pin_memory(),
-              torch.empty(PL, dtype=torch.int64).pin_memory())
-        for _ in range(max(1, args.warmup)):
+    # -- end to end with pinned host buffers ----------------------------------------
+    # N = 1: one mp_selfjoin call on host pointers (it copies in and out itself).
+    # N > 1: every rank copies the series in, joins its diagonal partitions and
+    # merges through one all-gather (shard.distributed_selfjoin); rank 0 reads
+    # the profile back.  Timed per rank with CUDA events, max over ranks.
+    xh = torch.from_numpy(x).pin_memory()
+    oh = (torch.empty(PL, dtype=torch.float64).pin_memory(),
+          torch.empty(PL, dtype=torch.int64).pin_memory())
+    xdev = torch.empty(n, dtype=torch.float64, device=dev)
+    parts = [(torch.empty(PL, dtype=torch.float64, device=dev),
+              torch.empty(PL, dtype=torch.int64, device=dev)) for _ in range(2)]
+
+    def e2e_step():
+        if world == 1:
             ctx.selfjoin(xh, m, precision=mp.FP32_REANCHOR, reanchor_k=args.reanchor_k, out=oh,
                          stream=stream.cuda_stream)
-        lat = []
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(2.0)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            ctx.selfjoin(xh, m, precision=mp.FP32_REANCHOR, reanchor_k=args.reanchor_k, out=oh,
-                         stream=stream.cuda_stream)
-            e1.record(stream)
-            e1.synchronize()
-            lat.append(e0.elapsed_time(e1))
-        e2e = {"value": cells_total * len(lat) / (sum(lat) * 1e-3), "unit": "cells/s",
-               "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 16 * PL,
-               "path": "mp_selfjoin (C ABI) with pinned host input/outputs"}
+            return
+        with torch.cuda.stream(stream):
+            xdev.copy_(xh, non_blocking=True)
+        used = [0]
+
+        def compute(a, b):
+            d, i = parts[used[0]]
+            used[0] += 1
+            ctx.selfjoin(xdev, m, precision=mp.FP32_REANCHOR, reanchor_k=args.reanchor_k,
+                         diag_lo=a, diag_hi=b, out=(d, i), stream=stream.cuda_stream)
+            return d, i
+
+        with torch.cuda.stream(stream):
+            md, mi = shard.distributed_selfjoin(compute, n, m)
+            if rank == 0:
+                oh[0].copy_(md, non_blocking=True)
+                oh[1].copy_(mi, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    lat = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(2.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_step()
+        e1.record(stream)
+        e1.synchronize()
+        lat.append(e0.elapsed_time(e1))
+    tot_e2e = sum(lat)
+    if world > 1:
+        t = torch.tensor([tot_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_e2e = float(t.item())
+    e2e = {"value": cells_total * len(lat) / (tot_e2e * 1e-3), "unit": "cells/s",
+           "h2d_bytes_per_step": 8 * n * world, "d2h_bytes_per_step": 16 * PL,
+           "path": "mp_selfjoin (C ABI) with pinned host input/outputs" if world == 1 else
+           f"pinned host series to each of {world} GPUs, mp_selfjoin per diagonal partition, "
+           "NCCL all-gather merge (shard.distributed_selfjoin), profile to pinned host on rank 0"}
 
     if rank != 0:
         ctx.close()
@@ -369,8 +404,7 @@ def run_ours(args, world):
         "gpu_launches": launches,
         "clocks": clocks,
     }
-    if e2e:
-        line["e2e"] = e2e
+    line["e2e"] = e2e
     if world == 1 and not args.no_cpu_baseline:
         threads = host_cores()
         cells, sec, kind, sample = cpu_reference_run(x, m, args.ref_seconds, threads)
