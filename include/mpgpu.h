@@ -47,7 +47,13 @@ typedef enum {
     MP_PREC_FP64 = 0,
     /* FP32 covariance recurrence re-anchored every reanchor_k steps by an FP64
      * dot product; window means/norms in FP64 (Welford). */
-    MP_PREC_FP32_REANCHOR = 1
+    MP_PREC_FP32_REANCHOR = 1,
+    /* MP_PREC_FP32_REANCHOR, except that tiles touching an ill-conditioned
+     * window -- flat, or with a norm over 16 times smaller than the largest
+     * norm among the reanchor_k + 256 windows before it (level steps, values
+     * beside constant stretches) -- run the same recurrence in FP64.  No
+     * window of a plain random walk qualifies, so there it costs nothing. */
+    MP_PREC_FP32_GUARDED = 2
 } mp_precision;
 
 typedef struct mp_context mp_context;

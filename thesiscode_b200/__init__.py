@@ -35,6 +35,7 @@ MP_ERR_NO_DEVICE = 6
 
 FP64 = 0
 FP32_REANCHOR = 1
+FP32_GUARDED = 2  # FP32 re-anchored with FP64 tiles around ill-conditioned windows
 
 FILETYPE_ASCII = 1
 FILETYPE_BIN = 2

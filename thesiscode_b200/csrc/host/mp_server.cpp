@@ -150,7 +150,9 @@ extern "C" {
 int mp_server_create(int device, size_t mem_budget_bytes, int slots, int precision,
                      int64_t reanchor_k, mp_server** out) {
     if (!out || slots < 1 || mem_budget_bytes == 0) return MP_ERR_INVALID_ARG;
-    if (precision != MP_PREC_FP64 && precision != MP_PREC_FP32_REANCHOR) return MP_ERR_INVALID_ARG;
+    if (precision != MP_PREC_FP64 && precision != MP_PREC_FP32_REANCHOR &&
+        precision != MP_PREC_FP32_GUARDED)
+        return MP_ERR_INVALID_ARG;
     mp_context* probe = nullptr;
     const int rc = mp_context_create(device, 0, &probe);
     if (rc != MP_OK) return rc;

@@ -213,6 +213,14 @@ size_t fp64_scratch(int64_t n, int64_t m, int64_t ndiag, bool host_io) {
     return b + 4096;
 }
 
+// Guarded form, on top of fp32_scratch: hazard prefix counts and scan
+// totals, block minima, FP64 recurrence terms.
+size_t guard_scratch(int64_t n, int64_t m) {
+    const int64_t PL = n - m + 1;
+    return align_up(4 * (size_t)(PL + 1)) + align_up(4 * (size_t)((PL + 1 + kThreads - 1) / kThreads + 1)) +
+           4 * align_up(8 * (size_t)PL) + 1024;
+}
+
 size_t fp32_scratch(int64_t n, int64_t m, bool host_io) {
     const int64_t PL = n - m + 1;
     size_t b = 0;
@@ -315,6 +323,7 @@ int64_t mp_last_launch_count(const mp_context* ctx) { return ctx ? ctx->launches
 size_t mp_selfjoin_scratch_bytes(int64_t n, int64_t m, int precision) {
     if (m < 2 || n < m) return 0;
     if (precision == MP_PREC_FP64) return fp64_scratch(n, m, n - m + 1, true);
+    if (precision == MP_PREC_FP32_GUARDED) return fp32_scratch(n, m, true) + guard_scratch(n, m);
     return fp32_scratch(n, m, true);
 }
 
@@ -324,7 +333,8 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
     Sizes S;
     int rc = check_join_args(ctx, A, n, m, excl, diag_lo, diag_hi, dist2_out, idx_out, S);
     if (rc) return rc;
-    if (precision != MP_PREC_FP64 && precision != MP_PREC_FP32_REANCHOR)
+    if (precision != MP_PREC_FP64 && precision != MP_PREC_FP32_REANCHOR &&
+        precision != MP_PREC_FP32_GUARDED)
         return fail(ctx, MP_ERR_INVALID_ARG, "unknown precision %d", precision);
     MP_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = (cudaStream_t)stream;
@@ -412,7 +422,8 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
     // ---- FP32 re-anchored form ----------------------------------------------
     int64_t K = reanchor_k > 0 ? reanchor_k : 1024;
     K = ((K + kFp32R - 1) / kFp32R) * kFp32R;
-    rc = reserve(ctx, fp32_scratch(n, m, !o_dev));
+    const bool guarded = precision == MP_PREC_FP32_GUARDED;
+    rc = reserve(ctx, fp32_scratch(n, m, !o_dev) + (guarded ? guard_scratch(n, m) : 0));
     if (rc) return rc;
     Carve cv{(char*)ctx->arena};
     double* Apad = cv.take<double>(n + kFp32Pad);
@@ -470,10 +481,45 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
         fp32_tile_plan(PL, S.lo, S.hi, K, kFp32R, P.nbands, P.seg_per_pair, ntiles);
         P.tile_begin = 0;
         P.key = key;
+        if (guarded) {
+            // hazard windows (prefix counts over PL + 1 entries) and FP64 terms
+            int* hz = cv.take<int>(PL + 1);
+            const int64_t hblk = (PL + 1 + kThreads - 1) / kThreads;
+            int* htot = cv.take<int>(hblk + 1);
+            double* pre = cv.take<double>(PL);
+            double* suf = cv.take<double>(PL);
+            double* gdf = cv.take<double>(PL);
+            double* gdg = cv.take<double>(PL);
+            const int64_t blk = K + 32 * kFp32R + 1;  // look back K + 32R windows
+            const int64_t nb = (PL + blk - 1) / blk;
+            hazard_block_minima_kernel<<<(unsigned)((nb + 127) / 128), 128, 0, st>>>(norm, PL, blk,
+                                                                                  pre, suf);
+            MP_LAUNCHED(ctx);
+            hazard_flags_kernel<<<grid_for(PL + 1), kThreads, 0, st>>>(norm, pre, suf, PL, blk, hz);
+            MP_LAUNCHED(ctx);
+            scan_blocks_kernel<<<(unsigned)hblk, kThreads, 0, st>>>(hz, PL + 1, htot);
+            MP_LAUNCHED(ctx);
+            scan_totals_kernel<<<1, 1, 0, st>>>(htot, hblk);
+            MP_LAUNCHED(ctx);
+            scan_add_kernel<<<(unsigned)hblk, kThreads, 0, st>>>(hz, PL + 1, htot);
+            MP_LAUNCHED(ctx);
+            guard_terms_kernel<<<grid_for(PL), kThreads, 0, st>>>(Apad, m, PL, mean, gdf, gdg);
+            MP_LAUNCHED(ctx);
+            P.hazard = hz;
+            P.norm = norm;
+            P.df = gdf;
+            P.dg = gdg;
+        }
         MP_CUDA(ctx, cudaMemcpyAsync(desc, &P, sizeof P, cudaMemcpyHostToDevice, st));
         MP_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
         launch_fp32_join<kFp32R>(desc, 1, ntiles, counter, st);
         MP_LAUNCHED(ctx);
+        if (guarded) {
+            // the same tiles again: the FP64 pass evaluates those the FP32 pass skipped
+            MP_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
+            launch_fp64_guard<kFp32R>(desc, 1, ntiles, counter, st);
+            MP_LAUNCHED(ctx);
+        }
         // the descriptor copy above reads host stack memory: finish it before returning
         MP_CUDA(ctx, cudaStreamSynchronize(st));
     }

@@ -185,6 +185,8 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
     const int64_t j0 = seg * P.K;
     const int64_t j1 = min(j0 + P.K, jmax);
     if (j0 >= j1) return;
+    // guarded form: tiles touching a hazard window are evaluated in FP64
+    if (P.hazard && fp32_tile_hazardous(P, gb, j0, j1, 32 * R)) return;
     const float ulim = (float)(1.0 + 1.0 / (double)P.m);
 
     // cell (column j, diagonal g0 + d) is evaluated iff d < ghi_rel and
@@ -393,24 +395,12 @@ __global__ void __launch_bounds__(32 * kFp32WarpsPerBlock, MPGPU_FP32_MIN_BLOCKS
             else hi = mid - 1;
         }
         const Fp32TileParams P = series[lo];
-        // local tile -> band pair p, slot s; the pair's bands k and nbands-1-k
-        // have nearly complementary lengths, so pairs carry nearly equal tile
-        // counts.  Consecutive tiles are consecutive column segments of one
-        // band: tiles running together touch disjoint columns and rows.
-        const int64_t lt = tt - P.tile_begin;
-        const int64_t p = lt / P.seg_per_pair;
-        int64_t s = lt % P.seg_per_pair;
-        const int64_t span = 32 * R;
-        const int64_t nseg0 = (P.PL - (P.g_lo + p * span) + P.K - 1) / P.K;
-        if (s < nseg0) {
-            tile_fp32<R>(P, p, s, lane, ring, rring, cring);
-            continue;
-        }
-        s -= nseg0;
-        const int64_t p2 = P.nbands - 1 - p;
-        if (p2 <= p) continue;
-        const int64_t nseg1 = (P.PL - (P.g_lo + p2 * span) + P.K - 1) / P.K;
-        if (s < nseg1) tile_fp32<R>(P, p2, s, lane, ring, rring, cring);
+        // local tile -> band and column segment (band pairs of nearly equal
+        // tile counts); consecutive tiles are consecutive column segments of
+        // one band, so tiles running together touch disjoint columns and rows
+        int64_t band, seg;
+        if (fp32_tile_of(P, tt - P.tile_begin, 32 * R, band, seg))
+            tile_fp32<R>(P, band, seg, lane, ring, rring, cring);
     }
 }
 

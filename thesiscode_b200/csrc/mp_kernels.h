@@ -72,7 +72,45 @@ struct Fp32TileParams {
     int64_t seg_per_pair;  // tiles per band pair (k, nbands-1-k), max over pairs
     int64_t tile_begin;    // first tile of this series in the launch
     unsigned long long* key;  // [PL] (ordered u << 32 | neighbour), min-merged
+    // Guarded form only (all null otherwise): hazard[w] = number of hazard
+    // windows among [0, w) (PL + 1 entries); FP64 inverse norms and
+    // recurrence terms for the FP64 tiles.
+    const int* hazard;
+    const double* norm;
+    const double* df;
+    const double* dg;
 };
+#ifdef __CUDACC__
+// Local tile lt of a series -> (band, column segment): band pair p = lt /
+// seg_per_pair holds bands p and nbands-1-p, whose lengths are nearly
+// complementary; the pair's tiles are its first band's segments, then the
+// second's.  False for the unused tail of a pair.
+__device__ __forceinline__ bool fp32_tile_of(const Fp32TileParams& P, int64_t lt, int64_t span,
+                                             int64_t& band, int64_t& seg) {
+    const int64_t p = lt / P.seg_per_pair;
+    int64_t s = lt % P.seg_per_pair;
+    const int64_t nseg0 = (P.PL - (P.g_lo + p * span) + P.K - 1) / P.K;
+    if (s < nseg0) {
+        band = p;
+        seg = s;
+        return true;
+    }
+    s -= nseg0;
+    const int64_t p2 = P.nbands - 1 - p;
+    if (p2 <= p) return false;
+    const int64_t nseg1 = (P.PL - (P.g_lo + p2 * span) + P.K - 1) / P.K;
+    band = p2;
+    seg = s;
+    return s < nseg1;
+}
+// Guarded form: does the tile (band start gb, columns [j0, j1)) touch a
+// hazard window, as a column or as a row (rows j + g, g in [gb, gb + span))?
+__device__ __forceinline__ bool fp32_tile_hazardous(const Fp32TileParams& P, int64_t gb, int64_t j0,
+                                                    int64_t j1, int span) {
+    const int64_t rs = min(j0 + gb, P.PL), re = min(j1 + gb + span, P.PL);
+    return (P.hazard[j1] - P.hazard[j0]) > 0 || (P.hazard[re] - P.hazard[rs]) > 0;
+}
+#endif
 // Persistent launch over `nseries` descriptors (device array) holding `total`
 // tiles; warps take tiles from *counter (zeroed by the caller beforehand).
 template <int R>
@@ -80,6 +118,18 @@ void launch_fp32_join(const Fp32TileParams* series_dev, int nseries, int64_t tot
                       unsigned long long* counter, cudaStream_t s);
 template <int R>
 void configure_fp32_join();
+// Guarded form (mp_guard.cu): hazard windows and the FP64 pass over their tiles.
+__global__ void hazard_block_minima_kernel(const double* nn, int64_t PL, int64_t blk, double* pre,
+                                           double* suf);
+__global__ void hazard_flags_kernel(const double* nn, const double* pre, const double* suf,
+                                    int64_t PL, int64_t blk, int* flag);
+__global__ void guard_terms_kernel(const double* A, int64_t m, int64_t PL, const double* mean,
+                                   double* df, double* dg);
+// Persistent FP64 pass over the same tile space as launch_fp32_join; only
+// tiles that touch a hazard window do work (counter zeroed beforehand).
+template <int R>
+void launch_fp64_guard(const Fp32TileParams* series_dev, int nseries, int64_t total,
+                       unsigned long long* counter, cudaStream_t s);
 // Tile count and seg_per_pair of one series (host helper).
 void fp32_tile_plan(int64_t PL, int64_t g_lo, int64_t g_hi, int64_t K, int R, int64_t& nbands,
                     int64_t& seg_per_pair, int64_t& ntiles);

@@ -156,7 +156,7 @@ def compare(x, m, segs, p64, p32, zero_level: bool, tol: float = 1e-4, K: int = 
     return rep
 
 
-def run(names, ks, device: int = 0, out=sys.stdout):
+def run(names, ks, device: int = 0, out=sys.stdout, forms=("fp32",)):
     with mp.Context(device) as ctx:
         ctx.set_phase_timing(True)
         for name in names:
@@ -166,10 +166,11 @@ def run(names, ks, device: int = 0, out=sys.stdout):
             p64 = ctx.selfjoin(x, m, precision=mp.FP64)
             wall64 = time.perf_counter() - t0
             join64 = ctx.last_phase_ms()[1]
-            for k in ks:
-                p32 = ctx.selfjoin(x, m, precision=mp.FP32_REANCHOR, reanchor_k=k)
+            for form, k in [(f, k) for f in forms for k in ks]:
+                prec = mp.FP32_GUARDED if form == "guarded" else mp.FP32_REANCHOR
+                p32 = ctx.selfjoin(x, m, precision=prec, reanchor_k=k)
                 join32 = ctx.last_phase_ms()[1]
-                rep = {"workload": name, "description": desc, "m": m, "reanchor_k": k,
+                rep = {"workload": name, "form": form, "description": desc, "m": m, "reanchor_k": k,
                        "cells": cells,
                        "fp64_join_ms": join64, "fp64_wall_s": wall64,
                        "fp32_join_ms": join32,
@@ -185,6 +186,9 @@ def main(argv=None):
     ap.add_argument("--ks", nargs="+", type=int, default=[64, 256, 1024])
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--out", default=None, help="append JSON lines here too")
+    ap.add_argument("--forms", nargs="+", default=["fp32"], choices=["fp32", "guarded"],
+                    help="fp32: the re-anchored form; guarded: with FP64 tiles around "
+                         "ill-conditioned windows")
     a = ap.parse_args(argv)
     if a.out:
         with open(a.out, "a") as f:
@@ -196,9 +200,9 @@ def main(argv=None):
                 def flush(self):
                     sys.stdout.flush()
                     f.flush()
-            run(a.workloads, a.ks, a.device, Tee())
+            run(a.workloads, a.ks, a.device, Tee(), tuple(a.forms))
     else:
-        run(a.workloads, a.ks, a.device)
+        run(a.workloads, a.ks, a.device, forms=tuple(a.forms))
 
 
 if __name__ == "__main__":
