@@ -48,11 +48,14 @@ typedef enum {
     /* FP32 covariance recurrence re-anchored every reanchor_k steps by an FP64
      * dot product; window means/norms in FP64 (Welford). */
     MP_PREC_FP32_REANCHOR = 1,
-    /* MP_PREC_FP32_REANCHOR, except that tiles touching an ill-conditioned
-     * window -- flat, or with a norm over 16 times smaller than the largest
-     * norm among the reanchor_k + 256 windows before it (level steps, values
-     * beside constant stretches) -- run the same recurrence in FP64.  No
-     * window of a plain random walk qualifies, so there it costs nothing. */
+    /* MP_PREC_FP32_REANCHOR plus three FP64 safeguards for ill-conditioned
+     * data: tiles touching a window that is flat or has a norm over 16 times
+     * smaller than the largest norm among the reanchor_k + 256 windows before
+     * it (level steps, values beside constant stretches) run the recurrence
+     * in FP64; windows whose best FP32 distance is below the FP32 resolution
+     * floor (u = d^2/2m < 1e-3, near-duplicates) are recomputed pairwise in
+     * FP64; and every window's chosen pair gets its distance from a centred
+     * FP64 dot product.  On a plain random walk only the last step runs. */
     MP_PREC_FP32_GUARDED = 2
 } mp_precision;
 
@@ -123,6 +126,10 @@ int mp_first_qt(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
 
 /* Kernel launches the last call on ctx made (for launch accounting). */
 int64_t mp_last_launch_count(const mp_context* ctx);
+/* MP_PREC_FP32_GUARDED: windows whose best FP32 distance was below the FP32
+ * resolution floor (u = d^2/2m < 1e-3) and were recomputed pairwise in FP64 by
+ * the last mp_selfjoin on ctx (at most 131072; -1 for other forms). */
+int64_t mp_last_near_duplicates(const mp_context* ctx);
 
 /* Phase timing: with on != 0, mp_selfjoin records CUDA events on its stream
  * around its three phases (preparation, join kernel, finalisation);

@@ -50,6 +50,7 @@ EXPORTED_SYMBOLS = (
     "mp_batch_launch_count", "mp_batch_upload", "mp_batch_launch", "mp_batch_download",
     "mp_batch_run", "mp_server_create", "mp_server_submit", "mp_server_poll", "mp_server_collect",
     "mp_server_stats", "mp_server_destroy", "mp_selfjoin_fp32_noalloc", "mp_prescrimp",
+    "mp_last_near_duplicates",
 )
 
 
@@ -89,6 +90,8 @@ def load_library() -> ctypes.CDLL:
     L.mp_first_qt.argtypes = [_P, _P, _i64, _i64, _i64, _i64, _P, _P]
     L.mp_prescrimp.argtypes = [_P, _P, _i64, _i64, ctypes.c_double, _P, _P, _P]
     L.mp_last_launch_count.argtypes = [_P]
+    L.mp_last_near_duplicates.argtypes = [_P]
+    L.mp_last_near_duplicates.restype = _i64
     L.mp_last_launch_count.restype = _i64
     L.mp_set_phase_timing.argtypes = [_P, ctypes.c_int]
     L.mp_last_phase_ms.argtypes = [_P, ctypes.POINTER(ctypes.c_double),
@@ -220,6 +223,11 @@ class Context:
     @property
     def last_launch_count(self) -> int:
         return int(self._L.mp_last_launch_count(self._h))
+
+    @property
+    def last_near_duplicates(self) -> int:
+        """Guarded form: windows the last self-join recomputed pairwise in FP64."""
+        return int(self._L.mp_last_near_duplicates(self._h))
 
     def selfjoin(self, A, m: int, precision: int = FP64, reanchor_k: int = 0,
                  blocklen: int = 0, diag_lo: int = 0, diag_hi: int = 0, excl: int = -1,

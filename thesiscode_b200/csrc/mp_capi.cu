@@ -30,6 +30,7 @@ struct mp_context {
     bool timing = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     double phase_ms[3] = {-1.0, -1.0, -1.0};
+    int64_t near_duplicates = -1;  // guarded form: windows of the last near-duplicate pass
 };
 
 namespace mpgpu {
@@ -215,10 +216,16 @@ size_t fp64_scratch(int64_t n, int64_t m, int64_t ndiag, bool host_io) {
 
 // Guarded form, on top of fp32_scratch: hazard prefix counts and scan
 // totals, block minima, FP64 recurrence terms.
+// Near-duplicate pass: windows whose best FP32 u is below kNearDupU are
+// recomputed pairwise in FP64, at most kNearDupCap of them (cost
+// count^2 * m FP64 FMAs; above the cap the FP32 values stand).
+constexpr float kNearDupU = 1e-3f;
+constexpr int kNearDupCap = 1 << 17;
+
 size_t guard_scratch(int64_t n, int64_t m) {
     const int64_t PL = n - m + 1;
     return align_up(4 * (size_t)(PL + 1)) + align_up(4 * (size_t)((PL + 1 + kThreads - 1) / kThreads + 1)) +
-           4 * align_up(8 * (size_t)PL) + 1024;
+           4 * align_up(8 * (size_t)PL) + align_up(4 * (size_t)kNearDupCap) + 2048;
 }
 
 size_t fp32_scratch(int64_t n, int64_t m, bool host_io) {
@@ -319,6 +326,7 @@ const char* mp_last_error(const mp_context* ctx) {
 }
 
 int64_t mp_last_launch_count(const mp_context* ctx) { return ctx ? ctx->launches : -1; }
+int64_t mp_last_near_duplicates(const mp_context* ctx) { return ctx ? ctx->near_duplicates : -1; }
 
 size_t mp_selfjoin_scratch_bytes(int64_t n, int64_t m, int precision) {
     if (m < 2 || n < m) return 0;
@@ -339,6 +347,7 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
     MP_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = (cudaStream_t)stream;
     ctx->launches = 0;
+    ctx->near_duplicates = -1;
     const bool a_dev = on_device(A);
     const bool o_dev = on_device(dist2_out);
     if (on_device(idx_out) != o_dev)
@@ -519,13 +528,45 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
             MP_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
             launch_fp64_guard<kFp32R>(desc, 1, ntiles, counter, st);
             MP_LAUNCHED(ctx);
+            // near duplicates below the FP32 resolution floor: exact pairs among them
+            int* ndl = cv.take<int>(kNearDupCap);
+            int* ndc = cv.take<int>(1);
+            const unsigned long long init = (unsigned long long)host_ord_f32(ulim) << 32;
+            MP_CUDA(ctx, cudaMemsetAsync(ndc, 0, sizeof(int), st));
+            neardup_collect_kernel<<<grid_for(PL), kThreads, 0, st>>>(key, PL, kNearDupU, init, ndl,
+                                                                      ndc, kNearDupCap);
+            MP_LAUNCHED(ctx);
+            int nd = 0;
+            MP_CUDA(ctx, cudaMemcpyAsync(&nd, ndc, sizeof(int), cudaMemcpyDeviceToHost, st));
+            MP_CUDA(ctx, cudaStreamSynchronize(st));
+            ctx->near_duplicates = nd;
+            if (nd > 0 && nd <= kNearDupCap) {
+                neardup_reset_kernel<<<grid_for(nd), kThreads, 0, st>>>(ndl, nd, key, init);
+                MP_LAUNCHED(ctx);
+                NearDupParams N{};
+                N.A = Apad;
+                N.mean = mean;
+                N.norm = norm;
+                N.m = m;
+                N.PL = PL;
+                N.g_lo = S.lo;
+                N.g_hi = S.hi;
+                N.list = ndl;
+                N.count = nd;
+                N.key = key;
+                N.ulim = ulim;
+                const int64_t nt = ((int64_t)nd + 31) / 32;
+                neardup_pairs_kernel<<<(unsigned)(nt * nt), 256, 0, st>>>(N);
+                MP_LAUNCHED(ctx);
+            }
         }
         // the descriptor copy above reads host stack memory: finish it before returning
         MP_CUDA(ctx, cudaStreamSynchronize(st));
     }
     mark(ctx, 2, st);
-    finalize_fp32_kernel<<<grid_for(PL), kThreads, 0, st>>>(key, PL, (double)m, Apad, mean, norm, 0,
-                                                            d2, ix);
+    // guarded form: the chosen pair's distance from a centred FP64 dot product
+    finalize_fp32_kernel<<<grid_for(PL), kThreads, 0, st>>>(key, PL, (double)m, Apad, mean, norm,
+                                                            guarded ? 1 : 0, d2, ix);
     MP_LAUNCHED(ctx);
     mark(ctx, 3, st);
     if (!o_dev) {

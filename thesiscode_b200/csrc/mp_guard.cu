@@ -201,6 +201,104 @@ __global__ void guard_terms_kernel(const double* __restrict__ A, int64_t m, int6
     }
 }
 
+// ---- near-duplicate pass ----------------------------------------------------
+// Windows whose best FP32 u lies below the FP32 resolution floor (u formed by
+// cancellation carries an absolute error of ~1e-7..1e-6) are collected, their
+// keys reset, and every pair among them recomputed exactly: a near-duplicate's
+// best partner has a tiny u too, so it is in the same set.
+
+__global__ void neardup_collect_kernel(const unsigned long long* __restrict__ key, int64_t PL,
+                                       float tau, unsigned long long init, int* __restrict__ list,
+                                       int* __restrict__ count, int cap) {
+    for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < PL;
+         w += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned long long k = key[w];
+        if (k >= init) continue;  // no neighbour
+        if (unord_f32((unsigned)(k >> 32)) < tau) {
+            const int i = atomicAdd(count, 1);
+            if (i < cap) list[i] = (int)w;
+        }
+    }
+}
+
+__global__ void neardup_reset_kernel(const int* __restrict__ list, int count,
+                                     unsigned long long* __restrict__ key, unsigned long long init) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+        key[list[i]] = init;
+}
+
+// Tile (ti, tj) of the list x list pair square, 32 x 32 pairs, 2 x 2 per
+// thread: centred FP64 dot products, u = 1 - dot * nn_w * nn_v, min-merged
+// into the row window's key (the square holds both orders of every pair).
+__global__ void __launch_bounds__(256) neardup_pairs_kernel(const NearDupParams P) {
+    constexpr int TB = 32, KC = 32;
+    __shared__ double sr[TB][KC + 1];
+    __shared__ double sc[TB][KC + 1];
+    __shared__ unsigned long long rmin[TB][16];
+    const int64_t nt = (P.count + TB - 1) / TB;
+    const int64_t ti = blockIdx.x / nt, tj = blockIdx.x % nt;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    for (int64_t k0 = 0; k0 < P.m; k0 += KC) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < TB * KC; e += blockDim.x) {
+            const int q = e / KC, kk = e % KC;
+            const int64_t k = k0 + kk;
+            const int64_t ir = ti * TB + q, ic = tj * TB + q;
+            double vr = 0.0, vc = 0.0;
+            if (k < P.m && ir < P.count) {
+                const int64_t w = P.list[ir];
+                vr = P.A[w + k] - P.mean[w];
+            }
+            if (k < P.m && ic < P.count) {
+                const int64_t v = P.list[ic];
+                vc = P.A[v + k] - P.mean[v];
+            }
+            sr[q][kk] = vr;
+            sc[q][kk] = vc;
+        }
+        __syncthreads();
+        const int kn = (int)min((int64_t)KC, P.m - k0);
+        for (int kk = 0; kk < kn; ++kk) {
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+                    acc[a][c] = __fma_rn(sr[ty * 2 + a][kk], sc[tx * 2 + c][kk], acc[a][c]);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        const int64_t ir = ti * TB + ty * 2 + a;
+        unsigned long long best = kNoKey;
+        if (ir < P.count) {
+            const int64_t w = P.list[ir];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int64_t ic = tj * TB + tx * 2 + c;
+                if (ic >= P.count) continue;
+                const int64_t v = P.list[ic];
+                const int64_t g = w > v ? w - v : v - w;
+                if (g < P.g_lo || g >= P.g_hi) continue;
+                const double u = __fma_rn(-acc[a][c], P.norm[w] * P.norm[v], 1.0);
+                const float fu = (float)u;
+                if (fu < P.ulim) {
+                    const unsigned long long kk = guard_key(fu, v);
+                    best = kk < best ? kk : best;
+                }
+            }
+        }
+        rmin[ty * 2 + a][tx] = best;
+    }
+    __syncthreads();
+    if (threadIdx.x < TB) {
+        const int64_t ir = ti * TB + threadIdx.x;
+        unsigned long long best = kNoKey;
+        for (int x = 0; x < 16; ++x) best = rmin[threadIdx.x][x] < best ? rmin[threadIdx.x][x] : best;
+        if (ir < P.count && best != kNoKey) atomicMin(P.key + P.list[ir], best);
+    }
+}
+
 template <int R>
 void launch_fp64_guard(const Fp32TileParams* series_dev, int nseries, int64_t total,
                        unsigned long long* counter, cudaStream_t s) {

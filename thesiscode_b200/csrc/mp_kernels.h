@@ -130,6 +130,23 @@ __global__ void guard_terms_kernel(const double* A, int64_t m, int64_t PL, const
 template <int R>
 void launch_fp64_guard(const Fp32TileParams* series_dev, int nseries, int64_t total,
                        unsigned long long* counter, cudaStream_t s);
+// Near-duplicate pass of the guarded form (mp_guard.cu).
+struct NearDupParams {
+    const double* A;
+    const double* mean;
+    const double* norm;  // FP64 inverse norms (NaN: flat)
+    int64_t m, PL;
+    int64_t g_lo, g_hi;  // pairs on diagonals [g_lo, g_hi) only
+    const int* list;     // the collected windows
+    int64_t count;
+    unsigned long long* key;
+    float ulim;
+};
+__global__ void neardup_collect_kernel(const unsigned long long* key, int64_t PL, float tau,
+                                       unsigned long long init, int* list, int* count, int cap);
+__global__ void neardup_reset_kernel(const int* list, int count, unsigned long long* key,
+                                     unsigned long long init);
+__global__ void neardup_pairs_kernel(const NearDupParams P);
 // Tile count and seg_per_pair of one series (host helper).
 void fp32_tile_plan(int64_t PL, int64_t g_lo, int64_t g_hi, int64_t K, int R, int64_t& nbands,
                     int64_t& seg_per_pair, int64_t& ntiles);

@@ -16,8 +16,10 @@ of 0.  Every window whose two results differ by more than 1e-4 is therefore
 judged against the distances of the chosen pairs computed directly (centred
 two-pass FP64 dot products, independent of both forms): the window is
 "reference-inaccurate" when the FP64 value is more than 1e-6 away from the
-direct distance of its own pair, when that pair is flat, or when the FP64 form
-found no neighbour although the FP32 form's pair is a valid one.  Windows
+direct distance of its own pair, when that pair is flat, when the FP64 form
+found no neighbour although the FP32 form's pair is a valid one, or when the
+FP32 form's pair is closer than the FP64 form's (the reference's rounding hid
+the nearest neighbour).  Windows
 wholly inside a constant stretch ("pseudo-flat") are counted apart: the FP32
 form detects them as flat and gives them the flat result (d2 = 2m + 2, index
 0) that the reference gives exactly flat windows.
@@ -110,6 +112,9 @@ def compare(x, m, segs, p64, p32, zero_level: bool, tol: float = 1e-4, K: int = 
             ref_bad[i] = True
         if e64 is None and e32 is not None and np.isfinite(e32) and e32 < none * (1 - 1e-6):
             ref_bad[i] = True
+        if (e64 is not None and e32 is not None and np.isfinite(e64) and np.isfinite(e32)
+                and e32 < e64 * (1 - 1e-6)):
+            ref_bad[i] = True  # the other form found a closer neighbour than the reference
         if e32 is not None and np.isfinite(e32) and e32 > 0:
             worst_vs_direct = max(worst_vs_direct, abs(d32[i] - e32) / e32)
             if e64 is not None and np.isfinite(e64) and e32 > e64 * (1 + tol):
@@ -176,6 +181,8 @@ def run(names, ks, device: int = 0, out=sys.stdout, forms=("fp32",)):
                        "fp32_join_ms": join32,
                        "fp64_cells_per_s": cells / (join64 * 1e-3),
                        "fp32_cells_per_s": cells / (join32 * 1e-3)}
+                if form == "guarded":
+                    rep["near_duplicates_recomputed"] = ctx.last_near_duplicates
                 rep.update(compare(x, m, segs, p64, p32, name == "c3z", K=k))
                 print(json.dumps(rep), file=out, flush=True)
 
