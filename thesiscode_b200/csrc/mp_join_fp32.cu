@@ -28,6 +28,7 @@
 // Reference semantics kept: strict improvement over the initial score -1
 // (u < 1 + 1/m), NaN never wins (a zero-variance window has nn = NaN).
 #include <algorithm>
+#include <atomic>
 
 #include "mp_common.cuh"
 #include "mp_kernels.h"
@@ -432,10 +433,15 @@ void configure_fp32_join() {
 template <int R>
 void launch_fp32_join(const Fp32TileParams* series_dev, int nseries, int64_t total,
                       unsigned long long* counter, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
+    // the shared-memory limit is a per-device attribute; setting it is
+    // idempotent, so concurrent first launches (server threads) are harmless
+    static std::atomic<unsigned long long> configured{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(configured.load(std::memory_order_acquire) & bit)) {
         configure_fp32_join<R>();
-        configured = true;
+        configured.fetch_or(bit, std::memory_order_release);
     }
     const int64_t want = (total + kFp32WarpsPerBlock - 1) / kFp32WarpsPerBlock;
     const int64_t blocks = std::min<int64_t>(want, 148 * MPGPU_FP32_MIN_BLOCKS);

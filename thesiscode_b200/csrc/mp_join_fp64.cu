@@ -26,6 +26,8 @@
 // (the reference's triv_par balance rule, ScrimpTrivialPar.cpp:200-224).
 #include <float.h>
 
+#include <atomic>
+
 #include "mp_common.cuh"
 #include "mp_kernels.h"
 
@@ -315,10 +317,14 @@ void launch_fp64_band(const Fp64BandParams& P, cudaStream_t s) {
     const int64_t njobs = (P.nbands + 1) / 2;
     const int64_t blocks = (njobs + kFp64WarpsPerBlock - 1) / kFp64WarpsPerBlock;
     constexpr int smem = fp64_smem_bytes<R>();
-    static bool configured = false;
-    if (!configured) {
+    // per-device attribute, idempotent: see launch_fp32_join
+    static std::atomic<unsigned long long> configured{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(configured.load(std::memory_order_acquire) & bit)) {
         cudaFuncSetAttribute(fp64_band_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        configured = true;
+        configured.fetch_or(bit, std::memory_order_release);
     }
     if (blocks > 0) fp64_band_kernel<R><<<(unsigned)blocks, 32 * kFp64WarpsPerBlock, smem, s>>>(P);
 }
