@@ -364,19 +364,27 @@ class Batch:
     def launch(self, stream=None):
         self._check(self._L.mp_batch_launch(self._h, stream))
 
-    def download(self, stream=None) -> list[Profile]:
+    def outputs(self) -> list[Profile]:
+        """Output arrays for every series of the plan, to reuse across runs (fresh
+        arrays pay page faults on every download)."""
         pls = self.lengths - self.windows + 1
-        d2 = [np.empty(int(p)) for p in pls]
-        ix = [np.empty(int(p), dtype=np.int64) for p in pls]
+        return [Profile(np.empty(int(p)), np.empty(int(p), dtype=np.int64)) for p in pls]
+
+    def download(self, stream=None, out=None) -> list[Profile]:
+        """Copies the profiles to the host, into ``out`` (from outputs()) when given."""
+        if out is None:
+            out = self.outputs()
+        d2 = [p.dist2 for p in out]
+        ix = [p.index for p in out]
         dp = (ctypes.c_void_p * len(d2))(*[a.ctypes.data for a in d2])
         ip = (ctypes.c_void_p * len(ix))(*[a.ctypes.data for a in ix])
         self._check(self._L.mp_batch_download(self._h, dp, ip, stream))
         return [Profile(a, b) for a, b in zip(d2, ix)]
 
-    def run(self, series, stream=None) -> list[Profile]:
+    def run(self, series, stream=None, out=None) -> list[Profile]:
         self.upload(series, stream)
         self.launch(stream)
-        return self.download(stream)
+        return self.download(stream, out)
 
 
 class Server:

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/mpgpu.h"
@@ -174,6 +175,26 @@ struct mp_batch {
 };
 
 namespace {
+
+// Host copies between the caller's per-series arrays and the pinned staging
+// buffers run on several threads: one thread moves a few GB/s, and the
+// staging copies of a large batch are gigabytes.
+template <class F>
+void for_series_parallel(int64_t count, F body) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int64_t nt = std::min<int64_t>(std::min<unsigned>(hw, 16u), std::max<int64_t>(count, 1));
+    if (nt <= 1) {
+        for (int64_t s = 0; s < count; ++s) body(s);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int64_t t = 0; t < nt; ++t)
+        pool.emplace_back([&, t] {
+            for (int64_t s = t; s < count; s += nt) body(s);
+        });
+    for (auto& th : pool) th.join();
+}
+
 
 int enqueue_batch(mp_batch* b, cudaStream_t st) {
     const int maxy = (int)std::min<int64_t>(b->count, 65535);
@@ -347,8 +368,9 @@ int mp_batch_upload(mp_batch* b, const void* const* series, void* stream) {
         return MP_ERR_OUT_OF_MEMORY;
     }
     cudaStreamSynchronize(st);  // the staging buffer may still feed a previous copy
-    for (int64_t s = 0; s < b->count; ++s)
+    for_series_parallel(b->count, [&](int64_t s) {
         std::memcpy((char*)b->in_stage + esz * b->series[s].in_off, series[s], esz * b->series[s].n);
+    });
     if (cudaMemcpyAsync(b->d_in, b->in_stage, esz * b->in_elems, cudaMemcpyHostToDevice, st) !=
         cudaSuccess)
         return MP_ERR_CUDA;
@@ -404,11 +426,11 @@ int mp_batch_download(mp_batch* b, double* const* dist2_out, int64_t* const* idx
     if (cudaStreamSynchronize(st) != cudaSuccess) return MP_ERR_CUDA;
     const double* d2 = (const double*)b->out_stage;
     const int64_t* ix = (const int64_t*)(b->out_stage + 8 * b->k_elems);
-    for (int64_t s = 0; s < b->count; ++s) {
+    for_series_parallel(b->count, [&](int64_t s) {
         const BatchSeries& bs = b->series[s];
         if (dist2_out[s]) std::memcpy(dist2_out[s], d2 + bs.k_off, 8 * bs.PL);
         if (idx_out[s]) std::memcpy(idx_out[s], ix + bs.k_off, 8 * bs.PL);
-    }
+    });
     return MP_OK;
 }
 
