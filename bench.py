@@ -345,6 +345,14 @@ def run_ours(args, world):
            f"pinned host series to each of {world} GPUs, mp_selfjoin per diagonal partition, "
            "NCCL all-gather merge (shard.distributed_selfjoin), profile to pinned host on rank 0"}
 
+    # the FP64 form's phases on one more (untimed) call: preparation holds the
+    # reference-order statistics and the first dot products of every diagonal
+    phases64 = None
+    if world == 1:
+        ctx.selfjoin(xd, m, precision=mp.FP64, out=(d2b, ixb), stream=stream.cuda_stream)
+        pp, pj, pf = ctx.last_phase_ms()
+        phases64 = {"prep_ms": pp, "join_ms": pj, "finalize_ms": pf}
+
     if rank != 0:
         ctx.close()
         return
@@ -395,7 +403,11 @@ def run_ours(args, world):
         "fp64_baseline": {"value": value64, "unit": "cells/s", "ms_per_step": tot64 / fsteps,
                           "kernel": "fp64_band_kernel (reference arithmetic, bit-identical)",
                           "roofline_frac_f64": roof64 / peaks["f64_dfma"] if peaks["f64_dfma"]
-                          else None, "kernel_ms": join64},
+                          else None, "kernel_ms": join64, "phases": phases64},
+        # the reference logs "(PL - excl)^2 / t" as its throughput (ScrimpVertBlocked
+        # PERF_LOG); the same figure for this run, beside the true cell count
+        "reference_log_metric": {"value": float(PL - excl) ** 2 / (total_ms / args.steps * 1e-3),
+                                 "unit": "matrix entries/s, (PL - excl)^2 / t"},
         "speedup_vs_fp64": value / value64,
         "error_vs_fp64": err,
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))}
@@ -410,6 +422,9 @@ def run_ours(args, world):
         cells, sec, kind, sample = cpu_reference_run(x, m, args.ref_seconds, threads)
         line["cpu_baseline"] = {"value": cells / sec, "unit": "cells/s", "cores": threads,
                                 "kind": kind, "sample": sample}
+        c1, s1, k1, smp1 = cpu_reference_run(x, m, min(3.0, args.ref_seconds), 1)
+        line["cpu_baseline_1core"] = {"value": c1 / s1, "unit": "cells/s", "cores": 1, "kind": k1,
+                                      "sample": smp1}
     print(json.dumps(line), flush=True)
     ctx.close()
 
