@@ -41,6 +41,7 @@ def test_status_strings():
 def test_registry_lists_gpu_variants():
     names = mp.list_algorithms()
     assert "gpu_vert_blocked_fp64" in names and "gpu_vert_blocked_fp32k" in names
+    assert "gpu_scrimppp" in names
 
 
 def test_scratch_estimate_grows_with_n():
