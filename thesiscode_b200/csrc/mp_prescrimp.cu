@@ -5,7 +5,7 @@
 // from each query's best neighbour j, the diagonal j - i is walked s - 1 cells
 // forward and backward with the reference's running dot product.  The
 // reference computes the query rows by FFT convolution (FFTW); here each cell
-// is a direct FP64 dot product over the window, tiled so that a CTA serves 16
+// is a direct FP64 dot product over the window, tiled so that a CTA serves 32
 // queries x 256 windows from shared memory (m DFMA per cell, no FFT, and more
 // accurate than the FFT's rounding).  All updates are min-merges of 64-bit
 // keys, so the result does not depend on the (shuffled, in the reference)
@@ -19,7 +19,8 @@ namespace mpgpu {
 
 namespace {
 
-constexpr int kQB = 16;    // queries per CTA
+constexpr int kQB = 32;    // queries per CTA
+constexpr int kQT = kQB / 4;  // queries per thread
 constexpr int kJB = 256;   // windows per CTA
 constexpr int kKC = 32;    // window elements per shared-memory stage
 constexpr unsigned long long kNone = ~0ull;
@@ -69,9 +70,9 @@ __global__ void prescrimp_keys_init_kernel(unsigned long long* __restrict__ a, i
 }
 
 // Query rows: CTA b covers windows [wt*256, wt*256+256) and queries
-// [qt*16, qt*16+16), wt = b % window tiles, qt = b / window tiles (a 1-D grid,
-// so any number of queries fits).  Thread (ty, tx) accumulates 4 queries x 4
-// windows.
+// [qt*32, qt*32+32), wt = b % window tiles, qt = b / window tiles (a 1-D grid,
+// so any number of queries fits).  Thread (ty, tx) accumulates 8 queries x 4
+// windows (12 shared-memory reads per 32 FMAs).
 __global__ void __launch_bounds__(256) prescrimp_rows_kernel(const PreScrimpParams P) {
     __shared__ double sq[kQB][kKC + 1];
     __shared__ double sw[kJB + kKC];
@@ -83,9 +84,9 @@ __global__ void __launch_bounds__(256) prescrimp_rows_kernel(const PreScrimpPara
     const int64_t nwt = (P.PL + kJB - 1) / kJB;
     const int64_t j0 = ((int64_t)blockIdx.x % nwt) * kJB;
     const int64_t t0 = ((int64_t)blockIdx.x / nwt) * kQB;
-    double acc[4][4];
+    double acc[kQT][4];
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
+    for (int r = 0; r < kQT; ++r)
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
     for (int64_t k0 = 0; k0 < P.m; k0 += kKC) {
@@ -102,13 +103,13 @@ __global__ void __launch_bounds__(256) prescrimp_rows_kernel(const PreScrimpPara
         __syncthreads();
         const int kn = (int)min((int64_t)kKC, P.m - k0);
         for (int kk = 0; kk < kn; ++kk) {
-            double a[4], w[4];
+            double a[kQT], w[4];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) a[r] = sq[ty * 4 + r][kk];
+            for (int r = 0; r < kQT; ++r) a[r] = sq[ty * kQT + r][kk];
 #pragma unroll
             for (int c = 0; c < 4; ++c) w[c] = sw[tx * 4 + c + kk];
 #pragma unroll
-            for (int r = 0; r < 4; ++r)
+            for (int r = 0; r < kQT; ++r)
 #pragma unroll
                 for (int c = 0; c < 4; ++c) acc[r][c] = __fma_rn(a[r], w[c], acc[r][c]);
         }
@@ -116,21 +117,21 @@ __global__ void __launch_bounds__(256) prescrimp_rows_kernel(const PreScrimpPara
     // distances; per window the best of this thread's 4 queries, per query the
     // best of its 4 windows
     const double mm = (double)P.m;
-    double cb[4], rb[4];
-    int ci[4], ri[4];
+    double cb[4], rb[kQT];
+    int ci[4], ri[kQT];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
         cb[c] = DBL_MAX;
         ci[c] = -1;
     }
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
+    for (int r = 0; r < kQT; ++r) {
         rb[r] = DBL_MAX;
         ri[r] = -1;
     }
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        const int64_t t = t0 + ty * 4 + r;
+    for (int r = 0; r < kQT; ++r) {
+        const int64_t t = t0 + ty * kQT + r;
         if (t >= P.Q) continue;
         const int64_t i = t * P.step;
         const double mi = P.mean[i], si = P.sigma[i];
@@ -156,9 +157,9 @@ __global__ void __launch_bounds__(256) prescrimp_rows_kernel(const PreScrimpPara
         cidx[ty][tx * 4 + c] = ci[c];
     }
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        rbest[tx][ty * 4 + r] = rb[r];
-        ridx[tx][ty * 4 + r] = ri[r];
+    for (int r = 0; r < kQT; ++r) {
+        rbest[tx][ty * kQT + r] = rb[r];
+        ridx[tx][ty * kQT + r] = ri[r];
     }
     __syncthreads();
     // windows: one thread per window of the tile
@@ -173,7 +174,7 @@ __global__ void __launch_bounds__(256) prescrimp_rows_kernel(const PreScrimpPara
             }
         if (bi >= 0) merge(P.kex, P.kix, j0 + c, b, bi, P.idx_bits);
     }
-    // queries: the first 16 threads
+    // queries: the first 32 threads
     if (threadIdx.x < kQB) {
         const int q = threadIdx.x;
         const int64_t t = t0 + q;
