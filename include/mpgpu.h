@@ -239,7 +239,8 @@ int mp_selfjoin_fp32_noalloc(const double* A_dev, int64_t n, int64_t m, int64_t 
  * reference to rounding, not bit for bit, and every update is a min-merge
  * (independent of the reference's shuffled query order).
  *   A            n doubles, host or device memory.
- *   stride       the reference's --prescrimp-stride (s = floor(stride * m) >= 1).
+ *   stride       the reference's --prescrimp-stride (an integer there; fractions
+ *                are accepted here), s = floor(stride * m) >= 1.
  *   dist2_out    PL doubles, idx_out PL int64 (host or device, same space).
  * Synchronous on stream.
  */

@@ -1,15 +1,20 @@
 """CPU restatement of PreSCRIMP -- TEST INFRASTRUCTURE (the checker for
 mp_prescrimp; never part of the product path).
 
-Parity unpinned: the reference's PreSCRIMP (scrimppp/src/ScrimpppOrig.cpp:
-130-266) convolves with FFTW, which is not installed here, so the reference's
-own code for this phase cannot be built or run; this restatement follows its
-steps and is not checked against reference outputs.  Differences from the
-reference, shared with the GPU implementation: query rows are direct FP64 dot
-products (not FFT convolutions), and every update is a min-merge, so the
-result does not depend on the shuffled query order (the reference assigns a
-query's row minimum to its own entry, :209-210, which differs from a min-merge
-only by rounding).
+Pinned against the reference's own PreSCRIMP (scrimppp/src/ScrimpppOrig.cpp:
+130-266), built unchanged as oracle/_ref/scrimppp_ref_orig.  That code
+convolves with FFTW, which is not installed here; oracle/ref_fftw_stub.cpp
+stands in for the FFTW calls it makes.  tests/golden/prescrimp_ref.npz holds
+its outputs (tests/golden/make_prescrimp_golden.py) and
+tests/test_prescrimp_oracle.py holds this restatement to them: distances
+within 1e-9 relative (1e-6 at a 1e4 level offset, where the FFT's own rounding
+dominates), indices equal.  Differences from the reference, shared with the GPU
+implementation: query rows are direct FP64 dot products (not FFT
+convolutions), and every update is a min-merge, so the result does not depend
+on the shuffled query order (the reference assigns a query's row minimum to
+its own entry, :209-210, which differs from a min-merge only by rounding).  A
+flat query window (zero variance) leaves the reference's row minimum index
+uninitialised (:196-211); the restatement skips such a query's walk.
 """
 from __future__ import annotations
 

@@ -43,6 +43,17 @@ def golden_edges():
 
 
 @pytest.fixture(scope="session")
+def golden_prescrimp():
+    """The reference's PreSCRIMP outputs (tests/golden/make_prescrimp_golden.py):
+    {case: {"x", "m", "stride", "dist" (sqrt |d2|), "index"}}."""
+    z = np.load(os.path.join(GOLDEN, "prescrimp_ref.npz"))
+    cases = {}
+    for name in z["names"]:
+        cases[str(name)] = {f: z[f"{name}/{f}"] for f in ("x", "m", "stride", "dist", "index")}
+    return cases
+
+
+@pytest.fixture(scope="session")
 def digests():
     return json.load(open(os.path.join(GOLDEN, "digests.json")))
 

@@ -1,8 +1,10 @@
-"""PreSCRIMP on the GPU (mp_prescrimp) against the CPU restatement
-(oracle/prescrimp.py): same queries, same exclusion rule, same diagonal walks.
-Parity with the reference itself is unpinned (its PreSCRIMP needs FFTW), so
-values are compared within 1e-9 relative (direct dot products on both sides,
-summed in different orders) and a differing index must tie in distance."""
+"""PreSCRIMP on the GPU (mp_prescrimp) against the reference's own PreSCRIMP
+(golden outputs of ScrimpppOrig.cpp, tests/golden/prescrimp_ref.npz) and
+against the CPU restatement (oracle/prescrimp.py, itself pinned to those
+outputs): same queries, same exclusion rule, same diagonal walks.  Values are
+compared within 1e-9 relative (direct dot products on both sides, summed in
+different orders; the reference's FFT rows where its tolerance says so) and a
+differing index must tie in distance."""
 from __future__ import annotations
 
 import os
@@ -29,6 +31,15 @@ def _check(x, m, got, want):
         a = pair_distance(x, m, int(w), int(i_g[w]))
         b = pair_distance(x, m, int(w), int(i_w[w]))
         assert a == pytest.approx(b, rel=1e-9, abs=1e-12), (w, i_g[w], i_w[w])
+
+
+def test_prescrimp_matches_reference_golden(gpu_ctx, golden_prescrimp):
+    from test_prescrimp_oracle import check_against_reference, golden_rtol
+    for name, c in golden_prescrimp.items():
+        m, stride = int(c["m"]), int(c["stride"])
+        got = gpu_ctx.prescrimp(c["x"], m, float(stride))
+        check_against_reference(c["x"], m, got.dist2, got.index, c["dist"],
+                                c["index"].astype(np.int64), rtol=golden_rtol(name))
 
 
 @pytest.mark.parametrize("n,m,stride", [(5000, 64, 0.25), (8000, 100, 1.0), (3000, 50, 100.0),
