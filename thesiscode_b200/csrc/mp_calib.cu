@@ -78,7 +78,7 @@ extern "C" int mp_measure_fma_peak(int device, int which, double* flops_per_s) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    const int blocks = 148 * 8, threads = 256;
+    const int blocks = sm_count() * 8, threads = 256;
     const int iters = (which == 2) ? 2048 : 8192;
     double best = 0.0;
     for (int rep = 0; rep < 4; ++rep) {

@@ -72,7 +72,8 @@ int fail(mp_context* ctx, int code, const char* fmt, ...) {
 unsigned grid_for(int64_t count) {
     int64_t b = (count + kThreads - 1) / kThreads;
     if (b < 1) b = 1;
-    if (b > 148 * 32) b = 148 * 32;
+    const int64_t cap = (int64_t)sm_count() * 32;
+    if (b > cap) b = cap;
     return (unsigned)b;
 }
 
@@ -150,12 +151,13 @@ int fp64_shards(int64_t PL) {
 // Diagonals per lane: 8 amortises the per-column warp reduction best; fewer
 // only when the band count would leave SMs idle (>= 4 warps per SM wanted).
 int pick_fp64_R(int64_t ndiag) {
+    const int sms = sm_count();
     for (int R : {8, 4}) {
         const int64_t nb = (ndiag + 32 * R - 1) / (32 * R);
-        if ((nb + 1) / 2 >= 148 * 4) return R;
+        if ((nb + 1) / 2 >= (int64_t)sms * 4) return R;
     }
     const int64_t nb2 = (ndiag + 63) / 64;
-    return (nb2 + 1) / 2 >= 148 ? 2 : 1;
+    return (nb2 + 1) / 2 >= sms ? 2 : 1;
 }
 
 int launch_band(int R, const Fp64BandParams& P, cudaStream_t s) {

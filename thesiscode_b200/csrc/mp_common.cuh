@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ < 1000)
 #error "mpgpu is written for sm_100a (B200) only"
 #endif
@@ -11,6 +13,28 @@
 namespace mpgpu {
 
 constexpr unsigned kFullMask = 0xffffffffu;
+
+// Streaming multiprocessors of the current device (148 on a B200), read once
+// per device; persistent and grid-stride launches are sized in multiples of
+// it.  A failed query answers with the B200's count.
+inline int sm_count() {
+    constexpr int kB200Sms = 148;
+    static std::atomic<int> cached[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return kB200Sms;
+    }
+    if (dev < 0 || dev >= 64) return kB200Sms;
+    int v = cached[dev].load(std::memory_order_relaxed);
+    if (v > 0) return v;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
+        cudaGetLastError();
+        return kB200Sms;
+    }
+    cached[dev].store(v, std::memory_order_relaxed);
+    return v;
+}
 
 // ---------------------------------------------------------------------------
 // Keys.  A profile entry is merged across threads, warps and CTAs with plain

@@ -303,7 +303,7 @@ template <int R>
 void launch_fp64_guard(const Fp32TileParams* series_dev, int nseries, int64_t total,
                        unsigned long long* counter, cudaStream_t s) {
     const int64_t want = (total + 3) / 4;
-    const int64_t blocks = std::min<int64_t>(want, 148 * 8);
+    const int64_t blocks = std::min<int64_t>(want, (int64_t)sm_count() * 8);
     if (blocks > 0) fp64_guard_kernel<R><<<(unsigned)blocks, 128, 0, s>>>(series_dev, nseries, total, counter);
 }
 

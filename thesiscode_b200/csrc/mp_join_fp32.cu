@@ -444,7 +444,7 @@ void launch_fp32_join(const Fp32TileParams* series_dev, int nseries, int64_t tot
         configured.fetch_or(bit, std::memory_order_release);
     }
     const int64_t want = (total + kFp32WarpsPerBlock - 1) / kFp32WarpsPerBlock;
-    const int64_t blocks = std::min<int64_t>(want, 148 * MPGPU_FP32_MIN_BLOCKS);
+    const int64_t blocks = std::min<int64_t>(want, (int64_t)sm_count() * MPGPU_FP32_MIN_BLOCKS);
     if (blocks > 0)
         fp32_join_kernel<R><<<(unsigned)blocks, 32 * kFp32WarpsPerBlock, fp32_smem_bytes<R>(), s>>>(
             series_dev, nseries, total, counter);

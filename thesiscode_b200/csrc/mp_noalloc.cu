@@ -120,7 +120,7 @@ bool device_resident(const void* p) {
 
 unsigned grid_for(int64_t count) {
     const int64_t g = (count + kThreads - 1) / kThreads;
-    return (unsigned)std::min<int64_t>(std::max<int64_t>(g, 1), 148 * 32);
+    return (unsigned)std::min<int64_t>(std::max<int64_t>(g, 1), (int64_t)sm_count() * 32);
 }
 
 unsigned ordered_f32(float v) {
