@@ -267,8 +267,7 @@ int mp_batch_create(mp_context* ctx, int64_t count, const int64_t* lengths, cons
         P.PL = bs.PL;
         P.g_lo = m / 4 + 1;
         P.g_hi = bs.PL;
-        int64_t K = (reanchor_k && reanchor_k[s] > 0) ? reanchor_k[s] : 1024;
-        P.K = ((K + kR - 1) / kR) * kR;
+        P.K = reanchor_interval(reanchor_k ? reanchor_k[s] : 0, kR);
         int64_t nt = 0;
         fp32_tile_plan(bs.PL, P.g_lo, P.g_hi, P.K, kR, P.nbands, P.seg_per_pair, nt);
         if (P.g_hi <= P.g_lo) nt = 0;

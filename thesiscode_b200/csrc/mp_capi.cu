@@ -431,8 +431,7 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
     }
 
     // ---- FP32 re-anchored form ----------------------------------------------
-    int64_t K = reanchor_k > 0 ? reanchor_k : 1024;
-    K = ((K + kFp32R - 1) / kFp32R) * kFp32R;
+    const int64_t K = reanchor_interval(reanchor_k, kFp32R);
     const bool guarded = precision == MP_PREC_FP32_GUARDED;
     rc = reserve(ctx, fp32_scratch(n, m, !o_dev) + (guarded ? guard_scratch(n, m) : 0));
     if (rc) return rc;

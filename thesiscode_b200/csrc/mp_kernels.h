@@ -147,6 +147,15 @@ __global__ void neardup_collect_kernel(const unsigned long long* key, int64_t PL
 __global__ void neardup_reset_kernel(const int* list, int count, unsigned long long* key,
                                      unsigned long long init);
 __global__ void neardup_pairs_kernel(const NearDupParams P);
+// Re-anchor interval K (columns per FP32 tile) from the caller's value: 1024
+// when not positive, at most 2^31 (every profile is shorter, so a longer
+// interval changes nothing and the rounding below cannot overflow), rounded
+// up to a multiple of the R columns a chunk processes.
+inline int64_t reanchor_interval(int64_t k, int R) {
+    int64_t K = k > 0 ? k : 1024;
+    if (K > (int64_t(1) << 31)) K = int64_t(1) << 31;
+    return ((K + R - 1) / R) * R;
+}
 // Tile count and seg_per_pair of one series (host helper).
 void fp32_tile_plan(int64_t PL, int64_t g_lo, int64_t g_hi, int64_t K, int R, int64_t& nbands,
                     int64_t& seg_per_pair, int64_t& ntiles);

@@ -179,8 +179,7 @@ extern "C" int mp_selfjoin_fp32_noalloc(const double* A_dev, int64_t n, int64_t 
     const int64_t PL = n - m + 1, nblk = (n + kThreads - 1) / kThreads;
     const int64_t ex = excl < 0 ? m / 4 : excl;
     const int64_t lo = ex + 1, hi = PL;
-    int64_t K = reanchor_k > 0 ? reanchor_k : 1024;
-    K = ((K + kR - 1) / kR) * kR;
+    const int64_t K = reanchor_interval(reanchor_k, kR);
 
     // The scratch keeps whatever the previous call left in it.  Every region
     // read below is first written on this stream: the series copy and its
