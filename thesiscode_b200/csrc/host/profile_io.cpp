@@ -46,6 +46,25 @@ Header read_header(std::ifstream& f, uint32_t want_fmt, const std::string& path)
     return h;
 }
 
+// Payload elements of `width` bytes the file holds after the read position, so
+// that a header count is checked against the file before anything is allocated.
+uint64_t payload_elements(std::ifstream& f, uint64_t width) {
+    const std::streampos here = f.tellg();
+    f.seekg(0, std::ios::end);
+    const std::streampos end = f.tellg();
+    f.seekg(here);
+    return end > here ? (uint64_t)(end - here) / width : 0;
+}
+
+void check_count(std::ifstream& f, const Header& h, uint64_t width, const char* what,
+                 const std::string& path) {
+    const uint64_t have = payload_elements(f, width);
+    if (h.count > have)
+        throw std::runtime_error(std::string("truncated ") + what + " file " + path + ": header says " +
+                                 std::to_string(h.count) + " entries, the file holds " +
+                                 std::to_string(have));
+}
+
 }  // namespace
 
 std::vector<double> read_series_ascii(const std::string& path) {
@@ -61,6 +80,7 @@ std::vector<double> read_series_bin(const std::string& path) {
     std::ifstream f(path, std::ios::binary);
     if (!f.is_open()) throw std::runtime_error("Could not open input file " + path);
     const Header h = read_header(f, kFmtSeries, path);
+    check_count(f, h, sizeof(double), "series", path);
     std::vector<double> x(h.count);
     f.read(reinterpret_cast<char*>(x.data()), sizeof(double) * h.count);
     if (!f) throw std::runtime_error("truncated series file " + path);
@@ -102,6 +122,7 @@ void read_profile_bin(const std::string& path, std::vector<double>& d2, std::vec
     std::ifstream f(path, std::ios::binary);
     if (!f.is_open()) throw std::runtime_error("Could not open profile file " + path);
     const Header h = read_header(f, kFmtProfile, path);
+    check_count(f, h, 16, "profile", path);
     d2.resize(h.count);
     idx.resize(h.count);
     std::vector<char> buf(16 * (size_t)h.count);

@@ -59,17 +59,28 @@ def _is_binary(path: str, fmt: int) -> bool:
     return f0 == fmt and off == HEADER_BYTES
 
 
+def _read_binary(path: str, fmt_want: int, dtype, what: str) -> np.ndarray:
+    """The payload of a binary file in the reference's format, its header's
+    count checked against the file's size before anything is read."""
+    with open(path, "rb") as f:
+        head = f.read(16)
+        if len(head) < 16:
+            raise ValueError(f"{path}: no binary header")
+        fmt, off, count = struct.unpack("<IIQ", head)
+        if fmt != fmt_want or off != HEADER_BYTES:
+            raise ValueError(f"{path}: not a binary {what} file (format {fmt}, offset {off})")
+        width = np.dtype(dtype).itemsize
+        have = max(os.path.getsize(path) - off, 0) // width
+        if count > have:
+            raise ValueError(f"{path}: truncated ({have} of {count} {what} entries)")
+        f.seek(off)
+        return np.frombuffer(f.read(width * count), dtype=dtype).copy()
+
+
 def read_profile(path: str):
     """(distances, indices) of an ASCII or binary (format 1) profile file."""
     if _is_binary(path, FMT_PROFILE):
-        with open(path, "rb") as f:
-            fmt, off, count = struct.unpack("<IIQ", f.read(16))
-            if fmt != FMT_PROFILE or off != HEADER_BYTES:
-                raise ValueError(f"{path}: not a binary profile (format {fmt}, offset {off})")
-            f.seek(off)
-            rec = np.frombuffer(f.read(16 * count), dtype=[("d2", "<f8"), ("idx", "<u8")])
-        if rec.size != count:
-            raise ValueError(f"{path}: truncated ({rec.size} of {count} records)")
+        rec = _read_binary(path, FMT_PROFILE, [("d2", "<f8"), ("idx", "<u8")], "profile")
         return np.sqrt(np.abs(rec["d2"])), rec["idx"].astype(np.int64)
     dist, idx = [], []
     with open(path) as f:
@@ -86,10 +97,7 @@ def read_series(path: str) -> np.ndarray:
     """A time series from an ASCII file (whitespace-separated values) or a
     binary series file (format 2)."""
     if _is_binary(path, FMT_SERIES):
-        with open(path, "rb") as f:
-            fmt, off, count = struct.unpack("<IIQ", f.read(16))
-            f.seek(off)
-            return np.frombuffer(f.read(8 * count), dtype="<f8").copy()
+        return _read_binary(path, FMT_SERIES, "<f8", "series")
     with open(path) as f:
         return np.array(f.read().split(), dtype=np.float64)
 
