@@ -88,3 +88,56 @@ def test_gloo_sharded_join_equals_single_join(oracle, world):
     for rank, d2, ix in res:
         assert np.array_equal(d2, ref_d2), rank
         assert np.array_equal(ix, ref_ix), rank
+
+
+def _failing_worker(rank, world, port, bad_rank, q):
+    """Rank `bad_rank`'s part raises; every rank must learn of it from the
+    status exchange and raise ShardFailure, none may wait in the data
+    exchange (a short process-group timeout bounds the test if one does)."""
+    import datetime
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=30))
+    try:
+        n, m = 3000, 32
+        x = workloads.random_walk(n, 9)
+
+        def compute(lo, hi):
+            if rank == bad_rank:
+                raise RuntimeError("device scratch allocation failed")
+            from oracle.oracle import Oracle
+            d2, ix = Oracle().selfjoin(x, m, diag_lo=lo, diag_hi=hi, nthreads=1)
+            return torch.from_numpy(d2), torch.from_numpy(ix)
+
+        try:
+            shard.distributed_selfjoin(compute, n, m)
+            q.put((rank, "returned", None))
+        except shard.ShardFailure as e:
+            q.put((rank, "ShardFailure", e.failed_ranks))
+        except Exception as e:  # noqa: BLE001 - reported to the test
+            q.put((rank, type(e).__name__, str(e)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("bad_rank", [0, 1])
+def test_failed_rank_is_reported_on_every_rank(oracle, bad_rank):
+    world = 2
+    ctx = tmp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_worker, args=(r, world, port, bad_rank, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    try:
+        res = sorted(q.get(timeout=120) for _ in range(world))
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.terminate()
+    assert res == [(r, "ShardFailure", [bad_rank]) for r in range(world)]
+    assert all(p.exitcode == 0 for p in procs)
+

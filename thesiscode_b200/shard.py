@@ -9,6 +9,11 @@ min-by-distance operator (ScrimpTrivialPar.cpp:68-108, 346-357) -- merges them.
 Here the exchange is an all-gather over torch.distributed (NCCL between GPUs,
 gloo in CPU tests) followed by an element-wise arg-min; ties go to the smaller
 neighbour index so the result does not depend on rank order.
+
+A rank whose part fails (an error from the library, say out of device memory)
+still takes every collective step: the ranks first exchange a status flag, and
+if any part failed every rank raises ShardFailure naming the failed ranks, so
+no rank is left waiting in the data exchange.
 """
 from __future__ import annotations
 
@@ -58,24 +63,52 @@ def merge_profiles(d2s: Sequence, idxs: Sequence):
     return d2, ix
 
 
+class ShardFailure(RuntimeError):
+    """Raised on every rank when the part of a sharded join of any rank failed."""
+
+    def __init__(self, failed_ranks):
+        super().__init__(f"sharded self-join failed on rank(s) {failed_ranks}")
+        self.failed_ranks = list(failed_ranks)
+
+
+def _exchange_status(failed: bool, world: int, group, dist, torch):
+    """Ranks whose part failed, as seen by every rank (one all-gather of a flag)."""
+    if dist.get_backend(group) == "nccl":
+        dev = torch.device("cuda", torch.cuda.current_device())
+    else:
+        dev = torch.device("cpu")
+    flags = [torch.zeros(1, dtype=torch.int32, device=dev) for _ in range(world)]
+    dist.all_gather(flags, torch.tensor([int(failed)], dtype=torch.int32, device=dev), group=group)
+    return [r for r, f in enumerate(flags) if int(f.item())]
+
+
 def distributed_selfjoin(compute: Callable, n: int, m: int, group=None):
     """Runs this rank's diagonal ranges through `compute(diag_lo, diag_hi) ->
     (d2, idx)` (torch tensors of length PL on this rank's device), merges them
     locally, then across ranks with one all-gather.  Every rank returns the
-    full profile."""
+    full profile, or raises ShardFailure if any rank's part failed."""
     import torch
     import torch.distributed as dist
     world = dist.get_world_size(group) if dist.is_initialized() else 1
     rank = dist.get_rank(group) if dist.is_initialized() else 0
     ranges = rank_ranges(n, m, rank, world)
-    parts = [compute(a, b) for a, b in ranges]
-    if not parts:
-        PL = n - m + 1
-        parts = [(torch.full((PL,), 2.0 * m + 2.0, dtype=torch.float64),
-                  torch.zeros(PL, dtype=torch.int64))]
-    d2, ix = merge_profiles([p[0] for p in parts], [p[1] for p in parts])
+    error = None
+    try:
+        parts = [compute(a, b) for a, b in ranges]
+        if not parts:
+            PL = n - m + 1
+            parts = [(torch.full((PL,), 2.0 * m + 2.0, dtype=torch.float64),
+                      torch.zeros(PL, dtype=torch.int64))]
+        d2, ix = merge_profiles([p[0] for p in parts], [p[1] for p in parts])
+    except Exception as e:  # reported to every rank below, then re-raised
+        if world == 1:
+            raise
+        error = e
     if world == 1:
         return d2, ix
+    failed = _exchange_status(error is not None, world, group, dist, torch)
+    if failed:
+        raise ShardFailure(failed) from error
     gd = [torch.empty_like(d2) for _ in range(world)]
     gi = [torch.empty_like(ix) for _ in range(world)]
     dist.all_gather(gd, d2.contiguous(), group=group)
