@@ -33,7 +33,8 @@ typedef enum {
     MP_ERR_BUDGET = 3,        /* request exceeds the context's memory budget */
     MP_ERR_CUDA = 4,          /* a CUDA call failed; see mp_last_error() */
     MP_ERR_NOT_SUPPORTED = 5, /* size or option outside what is implemented */
-    MP_ERR_NO_DEVICE = 6      /* no usable sm_100 device */
+    MP_ERR_NO_DEVICE = 6,     /* no usable sm_100 device */
+    MP_ERR_IO = 7             /* a series or profile file could not be read or written */
 } mp_status;
 
 typedef enum {
@@ -260,6 +261,10 @@ int mp_measure_fma_peak(int device, int which, double* flops_per_s);
  * mp_run_algorithm runs one registered variant end to end on files, like the
  * reference's main (scrimppp/src/main.cpp:47-80): filetype 1 = ASCII,
  * 2 = binary; blocklen/reanchor_k <= 0 keep the defaults (500 / 1024).
+ * Returns MP_ERR_INVALID_ARG for an unknown name or bad parameters,
+ * MP_ERR_IO when the input cannot be read (checked before any device is
+ * used) or the output cannot be written, and otherwise the status of the
+ * failing library call (MP_ERR_NO_DEVICE without a B200, ...).
  */
 int mp_list_algorithms(char* buf, size_t len);
 int mp_run_algorithm(const char* algo, const char* input_file, const char* output_file,

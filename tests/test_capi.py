@@ -73,3 +73,66 @@ def test_cells_count():
     PL, excl = n - m + 1, m // 4
     assert mp.cells(n, m) == (PL - excl - 1) * (PL - excl) // 2
     assert mp.cells(n, m, 200, 300) == sum(PL - d for d in range(200, 300))
+
+
+def test_run_algorithm_statuses_without_a_device(tmp_path):
+    import torch
+    series = tmp_path / "x.ascii"
+    series.write_text("\n".join(str(v) for v in range(200)))
+    out = str(tmp_path / "out.ascii")
+    # unknown variant, then an unreadable input: both reported before any device use
+    assert mp.run_algorithm("no_such_variant", str(series), out, 16) == mp.MP_ERR_INVALID_ARG
+    assert mp.run_algorithm("gpu_vert_blocked_fp64", str(tmp_path / "missing.ascii"), out,
+                            16) == mp.MP_ERR_IO
+    assert "file" in mp.status_string(mp.MP_ERR_IO)
+    if not torch.cuda.is_available():
+        assert mp.run_algorithm("gpu_vert_blocked_fp64", str(series), out, 16) == mp.MP_ERR_NO_DEVICE
+
+
+def test_entry_points_reject_null_arguments():
+    import ctypes
+    L = mp.load_library()
+    buf = (ctypes.c_double * 8)()
+    ib = (ctypes.c_int64 * 8)()
+    p = ctypes.cast(buf, ctypes.c_void_p)
+    q = ctypes.cast(ib, ctypes.c_void_p)
+    E = mp.MP_ERR_INVALID_ARG
+    assert L.mp_selfjoin(None, p, 8, 4, -1, mp.FP64, 0, 0, 0, 0, p, q, None) == E
+    assert L.mp_prescrimp(None, p, 8, 4, 1.0, p, q, None) == E
+    assert L.mp_window_stats(None, p, 8, 4, p, p, None) == E
+    assert L.mp_first_qt(None, p, 8, 4, 0, 1, p, None) == E
+    assert L.mp_eval_diag_block_triangle(None, p, q, p, q, p, 1, 1, p, p, 4, p, p, p, p, 0, 0,
+                                         None) == E
+    assert L.mp_context_create(0, 0, None) == E
+    assert L.mp_context_destroy(None) == E
+    assert L.mp_last_error(None) == b"no context"
+    assert L.mp_last_launch_count(None) == -1 and L.mp_last_near_duplicates(None) == -1
+    assert L.mp_set_phase_timing(None, 1) == E
+    srv = ctypes.c_void_p()
+    assert L.mp_server_create(0, 0, 1, mp.FP32_REANCHOR, 0, ctypes.byref(srv)) == E  # no budget
+    assert L.mp_server_create(0, 1 << 30, 0, mp.FP32_REANCHOR, 0, ctypes.byref(srv)) == E  # no slot
+    assert L.mp_server_create(0, 1 << 30, 1, 7, 0, ctypes.byref(srv)) == E  # unknown form
+    assert L.mp_server_submit(None, p, 8, 4, ctypes.byref(ctypes.c_int64())) == E
+    assert L.mp_batch_create(None, 1, q, q, None, 0, ctypes.byref(srv)) == E
+    v = ctypes.c_double()
+    assert L.mp_measure_fma_peak(0, 3, ctypes.byref(v)) == E
+    assert L.mp_run_algorithm(None, b"x", b"y", 16, 0, 0, 1, 0, 0) == E
+
+
+def test_allocation_free_entry_checks_arguments_before_the_device():
+    import ctypes
+    L = mp.load_library()
+    L.mp_selfjoin_fp32_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                           ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p,
+                                           ctypes.c_size_t]
+    err = ctypes.create_string_buffer(256)
+    fake = ctypes.c_void_p(256)  # never dereferenced: the size checks come first
+    rc = L.mp_selfjoin_fp32_noalloc(None, 100, 10, -1, 0, fake, fake, None, err, 256)
+    assert rc == mp.MP_ERR_INVALID_ARG and b"null" in err.value
+    rc = L.mp_selfjoin_fp32_noalloc(fake, 100, 1, -1, 0, fake, fake, None, err, 256)
+    assert rc == mp.MP_ERR_INVALID_ARG and b"window length" in err.value
+    rc = L.mp_selfjoin_fp32_noalloc(fake, 5, 10, -1, 0, fake, fake, None, err, 256)
+    assert rc == mp.MP_ERR_INVALID_ARG and b"shorter" in err.value
+    rc = L.mp_selfjoin_fp32_noalloc(fake, 1 << 20, 10, -1, 0, fake, fake, None, err, 256)
+    assert rc == mp.MP_ERR_NOT_SUPPORTED and b"mp_selfjoin" in err.value

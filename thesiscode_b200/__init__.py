@@ -32,6 +32,7 @@ MP_ERR_BUDGET = 3
 MP_ERR_CUDA = 4
 MP_ERR_NOT_SUPPORTED = 5
 MP_ERR_NO_DEVICE = 6
+MP_ERR_IO = 7
 
 FP64 = 0
 FP32_REANCHOR = 1

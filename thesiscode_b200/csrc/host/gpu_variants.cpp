@@ -9,11 +9,13 @@
 //
 // Both read the series (ASCII or binary, ScrimpSequ.hpp:91-112), run one
 // self-join through mp_selfjoin and store the profile like
-// ScrimpSequ::store_matrix_profile (ScrimpSequ.cpp:375-309).
+// ScrimpSequ::store_matrix_profile (ScrimpSequ.cpp:253-309).
 #include <chrono>
 #include <cstring>
+#include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -26,17 +28,24 @@ namespace matrix_profile {
 
 namespace {
 
+// A failed library call, carrying its mp_status so that mp_run_algorithm
+// returns the status itself rather than a generic one.
+struct StatusError : std::runtime_error {
+    StatusError(int s, const std::string& what) : std::runtime_error(what), status(s) {}
+    int status;
+};
+
 std::vector<double> fetch_series(const Scrimppp_params& p) {
     switch (p.filetype) {
         case Scrimppp_params::ASCII: return io::read_series_ascii(p.time_series_filename);
         case Scrimppp_params::BIN: return io::read_series_bin(p.time_series_filename);
-        default: throw std::runtime_error("Unhandled file type detected.");
+        default: throw std::invalid_argument("Unhandled file type detected.");
     }
 }
 
 void store_profile(const Scrimppp_params& p, const std::vector<double>& d2,
                    const std::vector<int64_t>& idx) {
-    if (p.output_filename.empty()) throw std::runtime_error("Empty output file name specified!");
+    if (p.output_filename.empty()) throw std::invalid_argument("Empty output file name specified!");
     switch (p.filetype) {
         case Scrimppp_params::ASCII:
             io::write_profile_ascii(p.output_filename, d2.data(), idx.data(), (int64_t)d2.size());
@@ -44,7 +53,7 @@ void store_profile(const Scrimppp_params& p, const std::vector<double>& d2,
         case Scrimppp_params::BIN:
             io::write_profile_bin(p.output_filename, d2.data(), idx.data(), (int64_t)d2.size());
             break;
-        default: throw std::runtime_error("Unhandled file type detected.");
+        default: throw std::invalid_argument("Unhandled file type detected.");
     }
 }
 
@@ -58,7 +67,7 @@ public:
         if (ctx_) return;
         const int rc = mp_context_create(params.device, params.mem_budget_bytes, &ctx_);
         if (rc != MP_OK)
-            throw std::runtime_error(std::string("mp_context_create: ") + mp_status_string(rc));
+            throw StatusError(rc, std::string("mp_context_create: ") + mp_status_string(rc));
     }
     void compute_matrix_profile(const Scrimppp_params& params) override {
         initialize(params);
@@ -76,7 +85,7 @@ public:
         const double sec =
             std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (rc != MP_OK)
-            throw std::runtime_error(std::string("mp_selfjoin: ") + mp_status_string(rc) + ": " +
+            throw StatusError(rc, std::string("mp_selfjoin: ") + mp_status_string(rc) + ": " +
                                      mp_last_error(ctx_));
         const double excl = (double)(m / 4);
         const double tri = (double)PL - excl;
@@ -120,7 +129,7 @@ public:
         const std::vector<double> A = fetch_series(params);
         const int64_t n = (int64_t)A.size(), m = params.query_window_len;
         if (m < 2 || n < m)
-            throw std::runtime_error(
+            throw std::invalid_argument(
                 "ERROR: Time series is shorter than the window length, can not proceed");
         const int64_t PL = n - m + 1;
         std::vector<double> d2(PL);
@@ -129,13 +138,13 @@ public:
         const int rc = mp_prescrimp(context(), A.data(), n, m, (double)params.prescrimp_stride,
                                     d2.data(), idx.data(), nullptr);
         if (rc != MP_OK)
-            throw std::runtime_error(std::string("mp_prescrimp: ") + mp_status_string(rc) + ": " +
+            throw StatusError(rc, std::string("mp_prescrimp: ") + mp_status_string(rc) + ": " +
                                      mp_last_error(context()));
         std::clog << "Time for PreSCRIMP: " << std::setprecision(17)
                   << std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count()
                   << std::endl;
         if (params.output_filename.empty())
-            throw std::runtime_error("Empty output file name specified!");
+            throw std::invalid_argument("Empty output file name specified!");
         io::write_profile_ascii(params.output_filename + "_prescrimp", d2.data(), idx.data(), PL);
         GpuVertBlocked::compute_matrix_profile(params);
     }
@@ -149,8 +158,11 @@ FactoryRegistration<GpuVertBlockedFp32K> reg_fp32("gpu_vert_blocked_fp32k");
 
 }  // namespace matrix_profile
 
+using matrix_profile::IMatProfAlgo;
 using matrix_profile::MatProfImplFactory;
 using matrix_profile::Scrimppp_params;
+using matrix_profile::StatusError;
+namespace io = matrix_profile::io;
 
 extern "C" int mp_list_algorithms(char* buf, size_t len) {
     const std::string s = MatProfImplFactory::getInstance().get_available_implementations();
@@ -174,14 +186,31 @@ extern "C" int mp_run_algorithm(const char* algo, const char* input_file, const 
     p.filetype = filetype == 2 ? Scrimppp_params::BIN : Scrimppp_params::ASCII;
     if (reanchor_k > 0) p.reanchor_k = (long)reanchor_k;
     p.device = device;
+    std::unique_ptr<IMatProfAlgo> a;
     try {
-        auto a = MatProfImplFactory::getInstance().create(p.algo_name);
+        a = MatProfImplFactory::getInstance().create(p.algo_name);
+    } catch (const std::out_of_range&) {
+        std::cerr << "mp_run_algorithm: unknown algorithm " << p.algo_name << std::endl;
+        return MP_ERR_INVALID_ARG;
+    }
+    // an unreadable input is reported before any device is touched
+    if (!std::ifstream(p.time_series_filename).good()) {
+        std::cerr << "mp_run_algorithm: Could not open input file " << p.time_series_filename
+                  << std::endl;
+        return MP_ERR_IO;
+    }
+    try {
         a->initialize(p);
         a->compute_matrix_profile(p);
         a->log_info();
-    } catch (const std::out_of_range&) {
-        return MP_ERR_INVALID_ARG;
-    } catch (const std::invalid_argument&) {
+    } catch (const StatusError& e) {
+        std::cerr << "mp_run_algorithm: " << e.what() << std::endl;
+        return e.status;
+    } catch (const io::IoError& e) {
+        std::cerr << "mp_run_algorithm: " << e.what() << std::endl;
+        return MP_ERR_IO;
+    } catch (const std::invalid_argument& e) {
+        std::cerr << "mp_run_algorithm: " << e.what() << std::endl;
         return MP_ERR_INVALID_ARG;
     } catch (const std::exception& e) {
         std::cerr << "mp_run_algorithm: " << e.what() << std::endl;

@@ -12,11 +12,18 @@
 #pragma once
 
 #include <cstdint>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
 namespace matrix_profile {
 namespace io {
+
+// A file that cannot be opened, read or written, or whose contents are not in
+// the expected format.
+struct IoError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
 
 std::vector<double> read_series_ascii(const std::string& path);
 std::vector<double> read_series_bin(const std::string& path);

@@ -289,6 +289,7 @@ const char* mp_status_string(int status) {
         case MP_ERR_CUDA: return "CUDA error";
         case MP_ERR_NOT_SUPPORTED: return "not supported";
         case MP_ERR_NO_DEVICE: return "no usable device";
+        case MP_ERR_IO: return "file could not be read or written";
         default: return "unknown status";
     }
 }
