@@ -3,8 +3,14 @@
 Replays workload c5 (arrivals at `rate` per second for `duration` seconds,
 lengths log-uniform in [1024, 1048576], m uniform in {32..1024}, seed 4):
 each request is submitted at its arrival time; a collector thread gathers
-finished profiles.  Reports p50/p99 latency (arrival to finish), admitted
-cells/s and rejections.
+finished profiles.  Reports p50/p99 latency from the scheduled arrival to the
+finished profile, admitted cells/s and rejections.
+
+The series are generated by a producer thread a bounded number of requests
+ahead of the submitter, so generating a long series does not hold back the
+arrivals behind it.  If the submitter still reaches an arrival late (the
+producer fell behind, or a submit took long), the lateness is added to that
+request's latency, so the figure always runs from the scheduled arrival.
 
     python -m thesiscode_b200.serve --rate 30 --duration 10
 """
@@ -12,6 +18,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import queue
 import threading
 import time
 
@@ -21,14 +28,31 @@ import thesiscode_b200 as mp
 from thesiscode_b200 import workloads
 
 
+def _producer(reqs, out: queue.Queue, stop: threading.Event):
+    for (_, n, _, s) in reqs:
+        x = workloads.random_walk(n, s)
+        while not stop.is_set():
+            try:
+                out.put(x, timeout=0.1)
+                break
+            except queue.Full:
+                continue
+        if stop.is_set():
+            return
+
+
 def run_stream(rate: float, duration: float, slots: int = 4, budget_gb: float = 64.0,
-               seed: int = 4, max_n: int | None = None, drain_timeout: float = 120.0):
+               seed: int = 4, max_n: int | None = None, drain_timeout: float = 120.0,
+               server=None, lookahead: int = 32):
+    """Replays the c5 stream at `rate` against `server` (a new mp.Server on
+    device 0 when None; any object with submit/done/collect/stats/close)."""
     reqs = workloads.c5_stream(rate, duration, seed)
     if max_n:
         reqs = [(t, min(n, max_n), m, s) for t, n, m, s in reqs]
-    series = {}
-    srv = mp.Server(0, int(budget_gb * (1 << 30)), slots, mp.FP32_REANCHOR, 1024)
+    own = server is None
+    srv = mp.Server(0, int(budget_gb * (1 << 30)), slots, mp.FP32_REANCHOR, 1024) if own else server
     tickets, lock = [], threading.Lock()
+    late = {}  # ticket -> seconds between the scheduled arrival and the submit
     lat, que, rejected = [], [], 0
     stop = threading.Event()
 
@@ -42,38 +66,52 @@ def run_stream(rate: float, duration: float, slots: int = 4, budget_gb: float = 
                     rc, _, l, q = srv.collect(t, want_profile=False)
                     with lock:
                         tickets.remove(t)
+                        d = late.pop(t, 0.0)
                     if rc == mp.MP_OK:
-                        lat.append(l)
-                        que.append(q)
+                        lat.append(l + d)
+                        que.append(q + d)
                     progressed = True
             if not progressed:
                 time.sleep(0.0005)
 
+    ready: queue.Queue = queue.Queue(maxsize=max(1, lookahead))
+    halt = threading.Event()
+    prod = threading.Thread(target=_producer, args=(reqs, ready, halt), daemon=True)
+    prod.start()
+    # the first arrivals' series are generated before the clock starts
+    while prod.is_alive() and ready.qsize() < min(lookahead, len(reqs)):
+        time.sleep(0.001)
     th = threading.Thread(target=collector, daemon=True)
     th.start()
     t0 = time.perf_counter()
     cells_submitted = 0.0
-    for (ta, n, m, s) in reqs:
-        x = series.get(s)
-        if x is None:
-            x = workloads.random_walk(n, s)
-        now = time.perf_counter() - t0
-        if ta > now:
-            time.sleep(ta - now)
-        t, rc = srv.submit(x, m)
-        if rc == mp.MP_ERR_BUDGET:
-            rejected += 1
-            srv.collect(t, want_profile=False)
-            continue
-        cells_submitted += mp.cells(n, m)
-        with lock:
-            tickets.append(t)
-    t_sub = time.perf_counter() - t0
-    stop.set()
-    th.join(timeout=drain_timeout)
-    t_end = time.perf_counter() - t0
-    st = srv.stats()
-    srv.close()
+    late_s = []
+    try:
+        for (ta, n, m, s) in reqs:
+            now = time.perf_counter() - t0
+            if ta > now:
+                time.sleep(ta - now)
+            x = ready.get()
+            d = max(0.0, time.perf_counter() - t0 - ta)
+            t, rc = srv.submit(x, m)
+            late_s.append(d)
+            if rc == mp.MP_ERR_BUDGET:
+                rejected += 1
+                srv.collect(t, want_profile=False)
+                continue
+            cells_submitted += mp.cells(n, m)
+            with lock:
+                late[t] = d
+                tickets.append(t)
+    finally:
+        halt.set()
+        t_sub = time.perf_counter() - t0
+        stop.set()
+        th.join(timeout=drain_timeout)
+        t_end = time.perf_counter() - t0
+        st = srv.stats()
+        if own:
+            srv.close()
     lat_ms = np.array(lat) * 1e3
     return {
         "rate_hz": rate, "duration_s": duration, "requests": len(reqs), "completed": len(lat),
@@ -81,7 +119,9 @@ def run_stream(rate: float, duration: float, slots: int = 4, budget_gb: float = 
         "p50_ms": float(np.percentile(lat_ms, 50)) if lat else None,
         "p99_ms": float(np.percentile(lat_ms, 99)) if lat else None,
         "queue_p50_ms": float(np.percentile(np.array(que) * 1e3, 50)) if que else None,
+        "submit_late_p99_ms": float(np.percentile(np.array(late_s) * 1e3, 99)) if late_s else None,
         "cells_per_s": st["cells"] / t_end if t_end > 0 else None,
+        "cells_submitted": cells_submitted,
         "submit_window_s": t_sub, "wall_s": t_end,
     }
 
