@@ -234,8 +234,12 @@ int mp_batch_create(mp_context* ctx, int64_t count, const int64_t* lengths, cons
     if (input_type != 0 && input_type != 1) return MP_ERR_INVALID_ARG;
     if (count > 65535) return MP_ERR_NOT_SUPPORTED;
     *out = nullptr;
-    int dev = 0;
-    cudaGetDevice(&dev);
+    // the batch lives on the context's device, whatever the caller's current one
+    const int dev = ctx_device(ctx);
+    if (cudaSetDevice(dev) != cudaSuccess) {
+        cudaGetLastError();
+        return MP_ERR_NO_DEVICE;
+    }
     mp_batch* b = new mp_batch();
     b->device = dev;
     b->input_f32 = input_type;
@@ -344,6 +348,7 @@ int mp_batch_create(mp_context* ctx, int64_t count, const int64_t* lengths, cons
 
 int mp_batch_destroy(mp_batch* b) {
     if (!b) return MP_ERR_INVALID_ARG;
+    cudaSetDevice(b->device);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     if (b->dev) cudaFree(b->dev);
@@ -359,6 +364,7 @@ int64_t mp_batch_launch_count(const mp_batch* b) { return b ? b->launches : 0; }
 
 int mp_batch_upload(mp_batch* b, const void* const* series, void* stream) {
     if (!b || !series) return MP_ERR_INVALID_ARG;
+    if (cudaSetDevice(b->device) != cudaSuccess) return MP_ERR_CUDA;
     cudaStream_t st = (cudaStream_t)stream;
     const size_t esz = b->input_f32 ? 4 : 8;
     if (!b->in_stage && cudaHostAlloc(&b->in_stage, esz * b->in_elems, 0) != cudaSuccess) {
@@ -378,6 +384,7 @@ int mp_batch_upload(mp_batch* b, const void* const* series, void* stream) {
 
 int mp_batch_launch(mp_batch* b, void* stream) {
     if (!b) return MP_ERR_INVALID_ARG;
+    if (cudaSetDevice(b->device) != cudaSuccess) return MP_ERR_CUDA;
     cudaStream_t st = (cudaStream_t)stream;
     if (!b->exec) {
         cudaStream_t cap = st;
@@ -387,8 +394,11 @@ int mp_batch_launch(mp_batch* b, void* stream) {
                 return MP_ERR_CUDA;
             own = true;
         }
-        if (cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        if (cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            if (own) cudaStreamDestroy(cap);
             return MP_ERR_CUDA;
+        }
         int rc = enqueue_batch(b, cap);
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(cap, &g);
@@ -411,6 +421,7 @@ int mp_batch_launch(mp_batch* b, void* stream) {
 
 int mp_batch_download(mp_batch* b, double* const* dist2_out, int64_t* const* idx_out, void* stream) {
     if (!b || !dist2_out || !idx_out) return MP_ERR_INVALID_ARG;
+    if (cudaSetDevice(b->device) != cudaSuccess) return MP_ERR_CUDA;
     cudaStream_t st = (cudaStream_t)stream;
     if (!b->out_stage && cudaHostAlloc((void**)&b->out_stage, 16 * b->k_elems, 0) != cudaSuccess) {
         cudaGetLastError();

@@ -35,6 +35,7 @@ struct mp_context {
 
 namespace mpgpu {
 size_t ctx_budget(const mp_context* ctx) { return ctx ? ctx->budget : 0; }
+int ctx_device(const mp_context* ctx) { return ctx ? ctx->device : 0; }
 }  // namespace mpgpu
 
 namespace {

@@ -11,6 +11,7 @@ namespace mpgpu {
 
 // Memory budget of a context (0 = none); defined with the context in mp_capi.cu.
 size_t ctx_budget(const mp_context* ctx);
+int ctx_device(const mp_context* ctx);
 
 // ---- preparation (mp_prep.cu) ----------------------------------------------
 __global__ void ref_prefix_kernel(const double* A, int64_t n, double* cs, double* cs2);
