@@ -85,8 +85,9 @@ struct Fp32TileParams {
 // Local tile lt of a series -> (band, column segment): band pair p = lt /
 // seg_per_pair holds bands p and nbands-1-p, whose lengths are nearly
 // complementary; the pair's tiles are its first band's segments, then the
-// second's.  False for the unused tail of a pair.
-__device__ __forceinline__ bool fp32_tile_of(const Fp32TileParams& P, int64_t lt, int64_t span,
+// second's.  False for the unused tail of a pair.  (Host-callable too, so the
+// tile space can be checked without a GPU.)
+__host__ __device__ __forceinline__ bool fp32_tile_of(const Fp32TileParams& P, int64_t lt, int64_t span,
                                              int64_t& band, int64_t& seg) {
     const int64_t p = lt / P.seg_per_pair;
     int64_t s = lt % P.seg_per_pair;
