@@ -1,0 +1,111 @@
+"""The FP64 form's index key (idx_key_f64, thesiscode_b200/csrc/mp_common.cuh)
+on CPU.  Profiles are max-merged on this 64-bit key, so it must order
+candidates by v = m - score (half the squared distance; smaller v wins), break
+equal high parts toward the smaller neighbour, put v <= 0 above every v > 0,
+keep ~33 mantissa bits at idx_bits = 24 (ties only within ~1.2e-10 relative),
+and give back the neighbour from its low bits.  Compiled with nvcc as a host
+program (the key function is host-callable)."""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CSRC = os.path.join(ROOT, "thesiscode_b200", "csrc")
+
+PROGRAM = r"""
+#include <cstdio>
+#include <random>
+#include "mp_common.cuh"
+using namespace mpgpu;
+
+static int fails = 0;
+#define CHECK(c, ...) do { if (!(c)) { if (fails++ < 10) { std::printf(__VA_ARGS__); std::printf("\n"); } } } while (0)
+
+static uint64_t nb_of(unsigned long long key, int idx_bits) {
+    const unsigned long long lowmask = (1ull << idx_bits) - 1ull;
+    return lowmask - (key & lowmask);
+}
+
+int main() {
+    std::mt19937_64 rng(12345);
+    for (int64_t m : {8LL, 64LL, 256LL, 400LL, 1024LL, 4096LL}) {
+        const long long vlo = key_vlo_bits(m);
+        // vlo = 2^(t-64) with 2^t > 2m + 2 >= 2^(t-1)
+        const int t = (int)((vlo >> 52) - 1023 + 64);
+        CHECK(std::ldexp(1.0, t) > 2.0 * m + 2.0 && std::ldexp(1.0, t - 1) <= 2.0 * m + 2.0,
+              "vlo m=%lld t=%d", (long long)m, t);
+        for (int idx_bits : {bits_for(1000), bits_for(1 << 20), bits_for((1 << 24) - 1)}) {
+            const uint64_t maxnb = (1ull << idx_bits) - 1;
+            std::uniform_real_distribution<double> U(-1.0, 1.0);
+            for (int it = 0; it < 20000; ++it) {
+                // two candidates' scores in [-m, m] (correlation in [-1, 1])
+                const double s1 = m * U(rng), s2 = m * U(rng);
+                const uint64_t n1 = rng() & maxnb, n2 = rng() & maxnb;
+                const unsigned long long k1 = idx_key_f64(s1, (double)m, n1, idx_bits, vlo);
+                const unsigned long long k2 = idx_key_f64(s2, (double)m, n2, idx_bits, vlo);
+                CHECK(nb_of(k1, idx_bits) == n1, "decode m=%lld", (long long)m);
+                const double v1 = m - s1, v2 = m - s2;
+                // clearly smaller v (beyond 2^-30 relative) -> larger key
+                if (v1 > 0 && v2 > 0 && v1 < v2 * (1.0 - std::ldexp(1.0, -30)))
+                    CHECK(k1 > k2, "order v1=%.17g v2=%.17g", v1, v2);
+                if (v1 <= 0 && v2 > 0) CHECK(k1 > k2, "region v1=%.17g v2=%.17g", v1, v2);
+            }
+            // equal scores: the smaller neighbour has the larger key
+            for (int it = 0; it < 2000; ++it) {
+                const double s = m * U(rng);
+                const uint64_t a = rng() & maxnb, b = rng() & maxnb;
+                if (a == b) continue;
+                const unsigned long long ka = idx_key_f64(s, (double)m, a, idx_bits, vlo);
+                const unsigned long long kb = idx_key_f64(s, (double)m, b, idx_bits, vlo);
+                CHECK((a < b) == (ka > kb), "tie s=%.17g a=%llu b=%llu", s,
+                      (unsigned long long)a, (unsigned long long)b);
+            }
+            // Resolution of the high part: 64 - idx_bits - 1 (region) - 6 (exponent)
+            // mantissa bits (33 at idx_bits = 24), i.e. |v|'s bit pattern in quanta
+            // of 2^(52 - mantissa bits).  Two v one quantum apart never share a high
+            // part.  The key sees v = m - score; score = -v with m = 0 keeps v exact.
+            const int mant = 64 - idx_bits - 1 - 6;
+            if (idx_bits == 24) CHECK(mant == 33, "mantissa bits %d", mant);
+            const long long quantum = 1ll << (52 - mant);
+            for (int it = 0; it < 20000; ++it) {
+                const double v = std::ldexp(1.0 + U(rng) * 0.5, -(int)(rng() % 30)) * m;
+                const long long b2 = f64_bits(v) + quantum;
+                double v2;
+                std::memcpy(&v2, &b2, sizeof v2);
+                const unsigned long long ka = idx_key_f64(-v, 0.0, 0, idx_bits, vlo);
+                const unsigned long long kb = idx_key_f64(-v2, 0.0, 0, idx_bits, vlo);
+                CHECK((ka >> idx_bits) > (kb >> idx_bits), "resolution v=%.17g", v);
+            }
+            // monotone across binade boundaries of v
+            for (int e = -40; e < t; ++e) {
+                const double below = std::nextafter(std::ldexp(1.0, e), 0.0);
+                const double at = std::ldexp(1.0, e);
+                if (at >= 2.0 * m + 2.0) break;
+                const unsigned long long kb_ = idx_key_f64(m - below, (double)m, 0, idx_bits, vlo);
+                const unsigned long long ka_ = idx_key_f64(m - at, (double)m, 0, idx_bits, vlo);
+                if (m - (m - below) < m - (m - at)) CHECK(kb_ >= ka_, "binade e=%d", e);
+            }
+        }
+    }
+    std::printf("%d failed\n", fails);
+    return fails ? 1 : 0;
+}
+"""
+
+
+def test_index_key_orders_and_decodes(tmp_path):
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not available")
+    src = tmp_path / "key.cu"
+    src.write_text(PROGRAM)
+    exe = tmp_path / "key"
+    subprocess.run([nvcc, "-std=c++17", "-O2", "-gencode", "arch=compute_100a,code=sm_100a",
+                    f"-I{CSRC}", str(src), "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "0 failed" in r.stdout

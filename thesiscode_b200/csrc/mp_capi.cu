@@ -119,21 +119,6 @@ bool on_device(const void* p) {
     return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
-// Lower end 2^(t-64) of the FP64 index key's distance range, as a bit
-// pattern, with 2^t > 2m + 2 >= every half squared distance m - score of a
-// candidate whose correlation is at least -1 (idx_key_f64).
-long long key_vlo_bits(int64_t m) {
-    int t = 1;
-    while (t < 62 && std::ldexp(1.0, t) <= 2.0 * (double)m + 2.0) ++t;
-    return (long long)(1023 + t - 64) << 52;
-}
-
-int bits_for(uint64_t maxval) {
-    int b = 1;
-    while (b < 63 && (1ull << b) <= maxval) ++b;
-    return b;
-}
-
 unsigned host_ord_f32(float v) {
     unsigned b;
     std::memcpy(&b, &v, 4);

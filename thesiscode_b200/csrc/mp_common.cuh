@@ -5,6 +5,8 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <cmath>
+#include <cstring>
 
 #if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ < 1000)
 #error "mpgpu is written for sm_100a (B200) only"
@@ -72,19 +74,45 @@ __device__ __forceinline__ float unord_f32(unsigned k) {
 // (33 mantissa bits at idx_bits = 24: candidates closer than ~1.2e-10 in
 // relative squared distance share a high part).  |v| outside [vlo, 2^t)
 // clamps to the range ends.
-__device__ __forceinline__ unsigned long long idx_key_f64(double score, double m,
-                                                          unsigned long long neighbour,
-                                                          int idx_bits, long long vlo_bits) {
+// Bit pattern of a double, on the host or the device.
+__host__ __device__ __forceinline__ long long f64_bits(double v) {
+#ifdef __CUDA_ARCH__
+    return __double_as_longlong(v);
+#else
+    long long b;
+    std::memcpy(&b, &v, sizeof b);
+    return b;
+#endif
+}
+
+__host__ __device__ __forceinline__ unsigned long long idx_key_f64(double score, double m,
+                                                                   unsigned long long neighbour,
+                                                                   int idx_bits, long long vlo_bits) {
     const unsigned long long lowmask = (1ull << idx_bits) - 1ull;
     const int shift = idx_bits > 5 ? idx_bits - 5 : 0;
     const long long span = 1ll << 58;  // 64 binades of 2^52 bit patterns
     const double v = m - score;
-    long long x = __double_as_longlong(fabs(v)) - vlo_bits;
+    long long x = f64_bits(fabs(v)) - vlo_bits;
     x = x < 0 ? 0 : (x > span - 1 ? span - 1 : x);
     const unsigned long long field =
         v > 0.0 ? (unsigned long long)(span - 1 - x) >> shift
                 : (1ull << (63 - idx_bits)) | ((unsigned long long)x >> shift);
     return (field << idx_bits) | (lowmask - neighbour);
+}
+
+// Host side of the index key: vlo_bits = the bit pattern of 2^(t-64), with
+// 2^t > 2m + 2 >= every half squared distance m - score of a candidate whose
+// correlation is at least -1; idx_bits = bits that hold every neighbour index
+// up to maxval.
+inline long long key_vlo_bits(int64_t m) {
+    int t = 1;
+    while (t < 62 && std::ldexp(1.0, t) <= 2.0 * (double)m + 2.0) ++t;
+    return (long long)(1023 + t - 64) << 52;
+}
+inline int bits_for(uint64_t maxval) {
+    int b = 1;
+    while (b < 63 && (1ull << b) <= maxval) ++b;
+    return b;
 }
 
 // ---------------------------------------------------------------------------
