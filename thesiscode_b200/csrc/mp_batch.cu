@@ -133,7 +133,6 @@ __global__ void batch_finalize_kernel(const BatchSeries* __restrict__ S,
     }
 }
 
-size_t al(size_t x) { return (x + 255) & ~size_t(255); }
 
 }  // namespace
 }  // namespace mpgpu
@@ -218,11 +217,6 @@ int enqueue_batch(mp_batch* b, cudaStream_t st) {
     return MP_OK;
 }
 
-unsigned host_ord_f32_b(float v) {
-    unsigned u;
-    std::memcpy(&u, &v, 4);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
 
 }  // namespace
 
@@ -288,9 +282,9 @@ int mp_batch_create(mp_context* ctx, int64_t count, const int64_t* lengths, cons
     b->k_elems = k;
     b->total_tiles = tiles;
     const size_t esz = input_type ? 4 : 8;
-    size_t bytes = al(sizeof(BatchSeries) * count) + al(sizeof(Fp32TileParams) * count) +
-                   al(4 * count) + al(8) + al(esz * in) + al(8 * a) + al(4 * a) + 2 * al(8 * w) +
-                   2 * al(32 * r) + al(8 * k) + al(8 * k) + al(8 * k);
+    size_t bytes = align_up(sizeof(BatchSeries) * count) + align_up(sizeof(Fp32TileParams) * count) +
+                   align_up(4 * count) + align_up(8) + align_up(esz * in) + align_up(8 * a) + align_up(4 * a) + 2 * align_up(8 * w) +
+                   2 * align_up(32 * r) + align_up(8 * k) + align_up(8 * k) + align_up(8 * k);
     if (ctx_budget(ctx) && bytes > ctx_budget(ctx)) {
         delete b;
         return MP_ERR_BUDGET;
@@ -304,7 +298,7 @@ int mp_batch_create(mp_context* ctx, int64_t count, const int64_t* lengths, cons
     char* p = b->dev;
     auto take = [&](size_t n) {
         char* q = p;
-        p += al(n);
+        p += align_up(n);
         return q;
     };
     b->d_series = (BatchSeries*)take(sizeof(BatchSeries) * count);
@@ -330,7 +324,7 @@ int mp_batch_create(mp_context* ctx, int64_t count, const int64_t* lengths, cons
         P.A = b->d_A + bs.a_off;
         P.mean = b->d_mean + bs.w_off;
         P.key = b->d_key + bs.k_off;
-        ulim[s] = host_ord_f32_b((float)(1.0 + 1.0 / (double)bs.m));
+        ulim[s] = host_ord_f32((float)(1.0 + 1.0 / (double)bs.m));
     }
     if (cudaMemcpy(b->d_series, b->series.data(), sizeof(BatchSeries) * count,
                    cudaMemcpyHostToDevice) != cudaSuccess ||

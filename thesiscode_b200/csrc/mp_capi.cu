@@ -70,15 +70,6 @@ int fail(mp_context* ctx, int code, const char* fmt, ...) {
             return fail(ctx, MP_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e_)); \
     } while (0)
 
-unsigned grid_for(int64_t count) {
-    int64_t b = (count + kThreads - 1) / kThreads;
-    if (b < 1) b = 1;
-    const int64_t cap = (int64_t)sm_count() * 32;
-    if (b > cap) b = cap;
-    return (unsigned)b;
-}
-
-size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Carves typed sub-buffers out of the context arena.
 struct Carve {
@@ -110,20 +101,6 @@ int reserve(mp_context* ctx, size_t bytes) {
     return MP_OK;
 }
 
-bool on_device(const void* p) {
-    cudaPointerAttributes at;
-    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
-}
-
-unsigned host_ord_f32(float v) {
-    unsigned b;
-    std::memcpy(&b, &v, 4);
-    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-}
 
 // Key shards spread the 64-bit max reductions of concurrently running bands
 // (which all walk the same columns) over more addresses; kept small enough

@@ -16,6 +16,30 @@ namespace mpgpu {
 
 constexpr unsigned kFullMask = 0xffffffffu;
 
+// ---------------------------------------------------------------------------
+// Host helpers shared by the entry points.
+// ---------------------------------------------------------------------------
+
+// Monotone map float -> uint32 on the host (the same map as ord_f32).
+inline unsigned host_ord_f32(float v) {
+    unsigned b;
+    std::memcpy(&b, &v, 4);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+// Sub-buffers of a scratch arena start on 256-byte boundaries.
+constexpr size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+// True for device (or managed) memory, false for host memory.
+inline bool on_device(const void* p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
 // Streaming multiprocessors of the current device (148 on a B200), read once
 // per device; persistent and grid-stride launches are sized in multiples of
 // it.  A failed query answers with the B200's count.
@@ -36,6 +60,15 @@ inline int sm_count() {
     }
     cached[dev].store(v, std::memory_order_relaxed);
     return v;
+}
+
+// Grid of a grid-stride launch of 256-thread blocks over `count` items: one
+// block per 256 items, at most 32 blocks per SM.
+inline unsigned grid_for(int64_t count) {
+    int64_t b = (count + 255) / 256;
+    if (b < 1) b = 1;
+    const int64_t cap = (int64_t)sm_count() * 32;
+    return (unsigned)(b > cap ? cap : b);
 }
 
 // ---------------------------------------------------------------------------

@@ -31,7 +31,6 @@ constexpr int64_t kPad = 64 * 8 + 64;   // zero padding behind the series and re
 constexpr int kThreads = 256;
 constexpr int kMaxDevices = 64;
 
-constexpr size_t al(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Carve-up of the scratch for a series of n samples (PL = n - m + 1 <= n).
 struct Layout {
@@ -40,16 +39,16 @@ struct Layout {
 constexpr Layout layout_for(int64_t n) {
     Layout L{};
     size_t o = 0;
-    L.a = o;       o += al(8 * (size_t)(n + kPad));                         // series + padding
-    L.chg = o;     o += al(4 * (size_t)n);                                  // change counts
-    L.tot = o;     o += al(4 * (size_t)((n + kThreads - 1) / kThreads + 1));
-    L.mean = o;    o += al(8 * (size_t)(n + kPad));
-    L.norm = o;    o += al(8 * (size_t)(n + kPad));
-    L.row = o;     o += al(32 * (size_t)(n + kPad));                        // row records
-    L.col = o;     o += al(32 * (size_t)(n + kPad));                        // column records
-    L.key = o;     o += al(8 * (size_t)n);                                  // profile keys
-    L.desc = o;    o += al(sizeof(Fp32TileParams));
-    L.counter = o; o += al(sizeof(unsigned long long));                     // tile counter
+    L.a = o;       o += align_up(8 * (size_t)(n + kPad));                         // series + padding
+    L.chg = o;     o += align_up(4 * (size_t)n);                                  // change counts
+    L.tot = o;     o += align_up(4 * (size_t)((n + kThreads - 1) / kThreads + 1));
+    L.mean = o;    o += align_up(8 * (size_t)(n + kPad));
+    L.norm = o;    o += align_up(8 * (size_t)(n + kPad));
+    L.row = o;     o += align_up(32 * (size_t)(n + kPad));                        // row records
+    L.col = o;     o += align_up(32 * (size_t)(n + kPad));                        // column records
+    L.key = o;     o += align_up(8 * (size_t)n);                                  // profile keys
+    L.desc = o;    o += align_up(sizeof(Fp32TileParams));
+    L.counter = o; o += align_up(sizeof(unsigned long long));                     // tile counter
     L.end = o;
     return L;
 }
@@ -109,25 +108,6 @@ int setup_current_device(void** out, char* err, size_t len) {
     return MP_OK;
 }
 
-bool device_resident(const void* p) {
-    cudaPointerAttributes at;
-    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
-}
-
-unsigned grid_for(int64_t count) {
-    const int64_t g = (count + kThreads - 1) / kThreads;
-    return (unsigned)std::min<int64_t>(std::max<int64_t>(g, 1), (int64_t)sm_count() * 32);
-}
-
-unsigned ordered_f32(float v) {
-    unsigned b;
-    std::memcpy(&b, &v, 4);
-    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-}
 
 // Writes the tile descriptor from a kernel argument, so that nothing on the
 // stream reads host memory after this function has returned.
@@ -158,7 +138,7 @@ extern "C" int mp_selfjoin_fp32_noalloc(const double* A_dev, int64_t n, int64_t 
     void* base = nullptr;
     int rc = setup_current_device(&base, err, err_len);
     if (rc != MP_OK) return rc;
-    if (!device_resident(A_dev) || !device_resident(dist2_dev) || !device_resident(idx_dev))
+    if (!on_device(A_dev) || !on_device(dist2_dev) || !on_device(idx_dev))
         return report(err, err_len, MP_ERR_INVALID_ARG,
                       "A, dist2 and idx must be device memory of the current device");
 
@@ -202,7 +182,7 @@ extern "C" int mp_selfjoin_fp32_noalloc(const double* A_dev, int64_t n, int64_t 
                                                                norm, rowrec, colrec);
     const float ulim = (float)(1.0 + 1.0 / (double)m);
     init_keys_kernel<<<grid_for(PL), kThreads, 0, st>>>(key, PL,
-                                                        (unsigned long long)ordered_f32(ulim) << 32);
+                                                        (unsigned long long)host_ord_f32(ulim) << 32);
     if (hi > lo) {
         Fp32TileParams P{};
         P.rowrec = rowrec;
