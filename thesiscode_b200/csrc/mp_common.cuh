@@ -97,16 +97,6 @@ __device__ __forceinline__ float unord_f32(unsigned k) {
     return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
 }
 
-// FP64 form, index key.  The low idx_bits hold (2^idx_bits - 1 - neighbour),
-// so that among equal high parts a max picks the smaller neighbour.  The high
-// 64 - idx_bits bits order candidates by v = m - score (half the squared
-// distance; exact by Sterbenz for score in [m/2, 2m]), smaller v higher: a
-// region bit (set for v <= 0) and then |v|'s bits taken relative to
-// vlo = 2^(t-64), where the host picks t with 2^t > 2m + 2, so that 64
-// binades need 6 exponent bits instead of 11 and the freed bits keep mantissa
-// (33 mantissa bits at idx_bits = 24: candidates closer than ~1.2e-10 in
-// relative squared distance share a high part).  |v| outside [vlo, 2^t)
-// clamps to the range ends.
 // Bit pattern of a double, on the host or the device.
 __host__ __device__ __forceinline__ long long f64_bits(double v) {
 #ifdef __CUDA_ARCH__
@@ -118,6 +108,16 @@ __host__ __device__ __forceinline__ long long f64_bits(double v) {
 #endif
 }
 
+// FP64 form, index key.  The low idx_bits hold (2^idx_bits - 1 - neighbour),
+// so that among equal high parts a max picks the smaller neighbour.  The high
+// 64 - idx_bits bits order candidates by v = m - score (half the squared
+// distance; exact by Sterbenz for score in [m/2, 2m]), smaller v higher: a
+// region bit (set for v <= 0) and then |v|'s bits taken relative to
+// vlo = 2^(t-64), where the host picks t with 2^t > 2m + 2, so that 64
+// binades need 6 exponent bits instead of 11 and the freed bits keep mantissa
+// (33 mantissa bits at idx_bits = 24: candidates closer than ~1.2e-10 in
+// relative squared distance share a high part).  |v| outside [vlo, 2^t)
+// clamps to the range ends.
 __host__ __device__ __forceinline__ unsigned long long idx_key_f64(double score, double m,
                                                                    unsigned long long neighbour,
                                                                    int idx_bits, long long vlo_bits) {
