@@ -65,15 +65,15 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device: int):
-        self.device = device
+    def __init__(self, device):
+        self.devices = [device] if isinstance(device, int) else list(device)
         self.proc = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.device)],
+                 "-lms", "200", "-i", ",".join(str(d) for d in self.devices)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -432,56 +432,90 @@ def run_ours(args, world):
 def run_batch_workload(args):
     """Workload c4: 4,096 FP32-input walks (lengths log-uniform in [2048,
     262144], m in {64, 128, 256}) solved by one persistent, graph-captured
-    launch per step; tile widths from the autotuner table."""
+    launch per step; tile widths from the autotuner table.  With --gpus N the
+    series are split into N groups of nearly equal cells (shard.balance_by_cost)
+    and each GPU runs its group as its own batch (replicas, nothing exchanged);
+    a step lasts until the slowest GPU is done."""
+    import threading
+
     import torch
 
     import thesiscode_b200 as mp
     import thesiscode_b200.workloads as wl
+    from thesiscode_b200 import shard
     data = wl.c4(args.c4_count)
     lens = [x.size for x, _ in data]
     ms = [m for _, m in data]
-    ctx = mp.Context(0)
-    b = mp.Batch(ctx, lens, ms, None, input_f32=True)
-    stream = torch.cuda.Stream()
-    b.upload([x for x, _ in data], stream.cuda_stream)
+    groups = shard.balance_by_cost([mp.cells(n, m) for n, m in zip(lens, ms)], max(1, args.gpus))
+    reps = []  # (context, batch, stream, series) per GPU with work
+    for d, g in enumerate(groups):
+        if not g:
+            continue
+        ctx = mp.Context(d)
+        b = mp.Batch(ctx, [lens[i] for i in g], [ms[i] for i in g], None, input_f32=True)
+        st = torch.cuda.Stream(device=d)
+        series = [data[i][0] for i in g]
+        b.upload(series, st.cuda_stream)
+        reps.append((ctx, b, st, series))
     for _ in range(args.warmup):
-        b.launch(stream.cuda_stream)
-    stream.synchronize()
-    evs = []
-    with ClockSampler(0) as clk:
+        for _, b, st, _ in reps:
+            b.launch(st.cuda_stream)
+    for _, _, st, _ in reps:
+        st.synchronize()
+    steps_ms = []
+    with ClockSampler([d for d, g in enumerate(groups) if g]) as clk:
         for _ in range(args.steps):
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            b.launch(stream.cuda_stream)
-            e1.record(stream)
-            evs.append((e0, e1))
-        stream.synchronize()
-    ms_step = float(np.mean([a.elapsed_time(c) for a, c in evs]))
+            evs = []
+            for _, b, st, _ in reps:
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                b.launch(st.cuda_stream)
+                e1.record(st)
+                evs.append((e0, e1))
+            for _, _, st, _ in reps:
+                st.synchronize()
+            steps_ms.append(max(a.elapsed_time(c) for a, c in evs))
+    ms_step = float(np.mean(steps_ms))
+    cells = sum(b.cells for _, b, _, _ in reps)
     # end to end through the public API: host series in, host profiles out,
-    # into output arrays allocated once (as a serving loop would keep them)
-    series = [x for x, _ in data]
-    out = b.outputs()
+    # into output arrays allocated once (as a serving loop would keep them);
+    # one host thread per GPU
+    outs = [b.outputs() for _, b, _, _ in reps]
+
+    def run_all():
+        ths = [threading.Thread(target=b.run, args=(series, st.cuda_stream), kwargs={"out": o})
+               for (_, b, st, series), o in zip(reps, outs)]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+
     for _ in range(max(1, args.warmup)):
-        b.run(series, stream.cuda_stream, out=out)
+        run_all()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        b.run(series, stream.cuda_stream, out=out)
+        run_all()
     e2e_s = (time.perf_counter() - t0) / args.steps
+    launches = sum(b.launch_count for _, b, _, _ in reps)
     line = {"metric": "batched self-join cells/s (c4, one persistent graph-captured launch)",
-            "value": b.cells / (ms_step * 1e-3), "unit": "cells/s", "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_step, "dtype": "f32", "data": "synthetic",
+            "value": cells / (ms_step * 1e-3), "unit": "cells/s", "n_gpus": len(reps),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "dtype": "f32",
+            "data": "synthetic", "scaling": "strong",
             "config": {"workload": f"c4: {len(data)} FP32 random walks, lengths log-uniform "
                                    f"[2048, 262144], m in {{64,128,256}}, seed 3",
-                       "series": len(data), "samples": int(sum(lens)), "cells": b.cells,
-                       "tiles": b.tiles, "launches_per_step": b.launch_count},
-            "e2e": {"value": b.cells / e2e_s, "unit": "cells/s",
+                       "series": len(data), "samples": int(sum(lens)), "cells": cells,
+                       "tiles": sum(b.tiles for _, b, _, _ in reps),
+                       "launches_per_step": launches,
+                       "parallelism": f"{len(reps)} replicas, series balanced by cells"},
+            "e2e": {"value": cells / e2e_s, "unit": "cells/s",
                     "h2d_bytes_per_step": 4 * int(sum(lens)),
                     "d2h_bytes_per_step": 16 * int(sum(l - m + 1 for l, m in zip(lens, ms)))},
-            "gpu_launches": b.launch_count * args.steps, "clocks": clk.summary()}
+            "gpu_launches": launches * args.steps, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
-    b.close()
-    ctx.close()
+    for ctx, b, _, _ in reps:
+        b.close()
+        ctx.close()
 
 
 def run_serving_workload(args):
@@ -489,8 +523,11 @@ def run_serving_workload(args):
     continuous-batching server; p50/p99 latency and admitted cells/s."""
     from thesiscode_b200.serve import run_stream
     for rate in args.rates:
-        r = run_stream(rate, args.serve_seconds, slots=args.slots)
+        # --gpus N: one server per GPU, requests handed out in turn
+        r = run_stream(rate, args.serve_seconds, slots=args.slots,
+                       devices=list(range(max(1, args.gpus))))
         r["metric"] = "serving p50/p99 solve latency (c5)"
+        r["n_gpus"] = max(1, args.gpus)
         print(json.dumps(r), flush=True)
 
 
@@ -514,6 +551,8 @@ def main():
     if args.impl == "reference":
         run_reference_arm(args, world)
         return
+    if args.workload in ("c4", "c5") and int(os.environ.get("RANK", "0")) != 0:
+        return  # replicas: rank 0 drives every GPU; the other ranks have no work
     if args.workload == "c4":
         run_batch_workload(args)
         return

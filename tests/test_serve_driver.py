@@ -80,3 +80,15 @@ def test_latency_counts_a_late_submitter():
     # the last submit happens ~n * 20 ms after the start, its arrival at <= 0.4 s
     assert r["submit_late_p99_ms"] > 0.5 * (n * 20.0 - 400.0)
     assert r["p99_ms"] >= r["submit_late_p99_ms"] * 0.9
+
+
+def test_replicas_take_requests_in_turn():
+    fakes = [FakeServer(service_s=0.002), FakeServer(service_s=0.002)]
+    r = serve.run_stream(100.0, 1.0, servers=fakes, max_n=20_000)
+    n = r["requests"]
+    assert r["replicas"] == 2 and r["requests_per_replica"] == [(n + 1) // 2, n // 2]
+    assert r["completed"] == n and not fakes[0].reqs and not fakes[1].reqs
+    reqs = workloads.c5_stream(100.0, 1.0)
+    want = [sum(mp.cells(min(nn, 20_000), m) for i, (_, nn, m, _) in enumerate(reqs) if i % 2 == k)
+            for k in range(2)]
+    assert [f.cells for f in fakes] == want

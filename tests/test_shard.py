@@ -141,3 +141,25 @@ def test_failed_rank_is_reported_on_every_rank(oracle, bad_rank):
     assert res == [(r, "ShardFailure", [bad_rank]) for r in range(world)]
     assert all(p.exitcode == 0 for p in procs)
 
+
+
+def test_balance_by_cost_for_batch_replicas():
+    data = workloads.c4(count=600)
+    costs = [shard_cells(x.size, m) for x, m in data]
+    for parts in (1, 2, 3, 8):
+        groups = shard.balance_by_cost(costs, parts)
+        assert sorted(i for g in groups for i in g) == list(range(len(costs)))
+        assert all(g == sorted(g) for g in groups)
+        loads = [sum(costs[i] for i in g) for g in groups]
+        # largest-first onto the least-loaded group: loads differ by at most one job
+        assert max(loads) - min(loads) <= max(costs)
+        if parts > 1:
+            assert max(loads) / min(loads) < 1.05
+    assert shard.balance_by_cost([5.0, 5.0], 4) == [[0], [1], [], []]
+    with pytest.raises(ValueError):
+        shard.balance_by_cost([1.0], 0)
+
+
+def shard_cells(n, m):
+    L = max(n - m + 1 - m // 4 - 1, 0)
+    return L * (L + 1) / 2

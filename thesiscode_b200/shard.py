@@ -46,6 +46,23 @@ def rank_ranges(n: int, m: int, rank: int, world: int, excl: int = -1) -> list[t
     return [(a, b) for a, b in mine if b > a]
 
 
+def balance_by_cost(costs: Sequence[float], parts: int) -> list[list[int]]:
+    """Indices of independent jobs (series of a batch) split into `parts`
+    groups of nearly equal total cost, for replicas on several GPUs: largest
+    job first, each onto the least-loaded group (ties: the lower group); each
+    group lists its indices in ascending order.  No job is split."""
+    if parts < 1:
+        raise ValueError("parts must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-float(costs[i]), i))
+    load = [0.0] * parts
+    groups: list[list[int]] = [[] for _ in range(parts)]
+    for i in order:
+        g = min(range(parts), key=lambda k: (load[k], k))
+        groups[g].append(i)
+        load[g] += float(costs[i])
+    return [sorted(g) for g in groups]
+
+
 def merge_profiles(d2s: Sequence, idxs: Sequence):
     """Element-wise arg-min over partial profiles (numpy or torch arrays):
     smaller squared distance wins, ties go to the smaller index."""
