@@ -40,15 +40,27 @@ def test_differing_indices_are_counted(oracle, tmp_path, capsys):
     assert validate.main(["compare", str(a), str(b)]) == 3
     out = capsys.readouterr().out
     assert "ERROR: Profile indices differ in 3 entries" in out
-    assert "l 4 has differing indices" in out
+    assert f"l 4 has differing indices, id1: {idx[3]} id2: {bad[3]}" in out
 
 
-def test_length_mismatch_fails(oracle, tmp_path):
+def test_length_mismatch_fails(oracle, tmp_path, capsys):
     x, m, d2, idx = _profile(oracle)
     a, b = tmp_path / "a.ascii", tmp_path / "b.ascii"
     validate.write_profile_ascii(str(a), d2, idx)
     validate.write_profile_ascii(str(b), d2[:-5], idx[:-5])
     assert validate.main(["compare", str(a), str(b), "--silent"]) == 5
+    assert "FATAL: file 2 is shorter than file 1!" in capsys.readouterr().out
+    assert validate.main(["compare", str(b), str(a), "--silent"]) == 5
+    assert "FATAL: file 1 is shorter than file 2!" in capsys.readouterr().out
+
+
+def test_reference_conversion_flags_are_accepted(oracle, tmp_path):
+    x, m, d2, idx = _profile(oracle)
+    a, b = tmp_path / "a.ascii", tmp_path / "b.bin"
+    validate.write_profile_ascii(str(a), d2, idx)
+    validate.write_profile_bin(str(b), d2, idx)
+    assert validate.main(["compare", str(a), str(b), "--silent", "--keep_converted",
+                          "--cvt_prof_path", "./cvt_matprof"]) == 0
 
 
 def test_equal_distance_neighbours_are_ties(oracle, tmp_path):

@@ -139,15 +139,20 @@ def compare_profiles(a, b, series=None, m: int | None = None, rel_tol: float = 1
     max_diff = float(np.nanmax(delta)) if n else 0.0
     return {"entries": n + length_diff, "index_differences": int(diff.size) - ties + length_diff,
             "ties_within_tolerance": ties, "length_difference": length_diff,
-            "max_abs_diff": max_diff, "differing_entries": diff}
+            "shorter": 0 if da.size == db.size else (2 if db.size < da.size else 1),
+            "max_abs_diff": max_diff, "differing_entries": diff,
+            "index_pairs": [(int(ia[i]), int(ib[i])) for i in diff[:1000]]}
 
 
 def _print_compare(rep, silent: bool) -> None:
+    # the messages of the reference's compare_profile_indices.py
     if not silent:
-        for i in rep["differing_entries"][:1000]:
-            print(f"l {i + 1} has differing indices")
-    if rep["length_difference"]:
-        print("FATAL: the profiles differ in length by %d entries" % rep["length_difference"])
+        for i, (x, y) in zip(rep["differing_entries"][:1000], rep["index_pairs"]):
+            print(f"l {i + 1} has differing indices, id1: {x} id2: {y}")
+    if rep["shorter"] == 2:
+        print("FATAL: file 2 is shorter than file 1!")
+    elif rep["shorter"] == 1:
+        print("FATAL: file 1 is shorter than file 2!")
     if rep["index_differences"] == 0:
         print("SUCCESS: The profile indices coincide in all %d entries" % rep["entries"])
     else:
@@ -237,9 +242,14 @@ def main(argv=None) -> int:
                                     "neighbours of equal distance")
     c.add_argument("--window", type=int, help="window length m (with --series)")
     c.add_argument("--rel-tol", type=float, default=1e-9)
+    # accepted for command-line compatibility with compare_profile_indices.py;
+    # binary profiles are read directly, so nothing is converted or kept
+    c.add_argument("--keep_converted", action="store_true", help=argparse.SUPPRESS)
+    c.add_argument("--cvt_prof_path", nargs=1, help=argparse.SUPPRESS)
     v = sub.add_parser("folder", help="validate all profiles of a validation job directory")
     v.add_argument("directory")
     v.add_argument("--force_orig_baseline", action="store_true")
+    v.add_argument("--cvt_prof_path", nargs=1, help=argparse.SUPPRESS)  # as in validate_profiles.py
     a = ap.parse_args(argv)
     if a.cmd == "compare":
         if a.series and not a.window:
