@@ -45,11 +45,13 @@ def golden_edges():
 @pytest.fixture(scope="session")
 def golden_prescrimp():
     """The reference's PreSCRIMP outputs (tests/golden/make_prescrimp_golden.py):
-    {case: {"x", "m", "stride", "dist" (sqrt |d2|), "index"}}."""
+    {case: {"x", "m", "stride", "dist" (sqrt |d2|), "index", "exact_dist", "exact_index"}};
+    dist/index are PreSCRIMP's profile, exact_* the final SCRIMP++ profile."""
     z = np.load(os.path.join(GOLDEN, "prescrimp_ref.npz"))
     cases = {}
     for name in z["names"]:
-        cases[str(name)] = {f: z[f"{name}/{f}"] for f in ("x", "m", "stride", "dist", "index")}
+        cases[str(name)] = {f: z[f"{name}/{f}"] for f in ("x", "m", "stride", "dist", "index",
+                                                           "exact_dist", "exact_index")}
     return cases
 
 

@@ -84,3 +84,24 @@ def test_cli_scrimppp_writes_prescrimp_and_exact_profiles(tmp_path, golden_ascii
     assert np.array_equal(exact[1], golden_ascii["idx_m64"])
     assert np.array_equal(exact[0], np.sqrt(np.abs(golden_ascii["d2_m64"])))
     assert os.path.getsize(str(out) + "_prescrimp") > 0
+
+
+@pytest.mark.parametrize("case", ["chirp_n2048_m64_s1", "walk_n1500_m50_s1"])
+def test_cli_scrimppp_final_profile_is_the_reference(tmp_path, golden_prescrimp, case):
+    # gpu_scrimppp's two files against the reference scrimppp_orig's; on the
+    # chirped sine hundreds of neighbours lie exactly m/4 away, where only
+    # PreSCRIMP looks
+    from test_prescrimp_oracle import check_against_reference, golden_rtol
+    from thesiscode_b200 import validate
+    c = golden_prescrimp[case]
+    x, m, stride = c["x"], int(c["m"]), int(c["stride"])
+    inp = tmp_path / "series.ascii"
+    inp.write_text(" ".join(repr(float(v)) for v in x))
+    out = tmp_path / "prof.ascii"
+    r = subprocess.run([mp.CLI_PATH, "gpu_scrimppp", str(m), str(stride), str(inp),
+                        "--output-file", str(out)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    for path, dist, index in ((str(out) + "_prescrimp", c["dist"], c["index"]),
+                              (str(out), c["exact_dist"], c["exact_index"])):
+        d, i = validate.read_profile(path)
+        check_against_reference(x, m, d * d, i, dist, index.astype(np.int64), rtol=golden_rtol(case))

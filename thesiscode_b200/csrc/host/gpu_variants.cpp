@@ -23,6 +23,7 @@
 #include "mpgpu.h"
 #include "matprof_algo.hpp"
 #include "profile_io.hpp"
+#include "scrimppp_merge.hpp"
 
 namespace matrix_profile {
 
@@ -76,9 +77,22 @@ public:
         if (m < 2 || n < m)
             throw std::invalid_argument(
                 "ERROR: Time series is shorter than the window length, can not proceed");
+        std::vector<double> d2;
+        std::vector<int64_t> idx;
+        join(params, A, d2, idx);
+        store_profile(params, d2, idx);
+    }
+
+protected:
+    mp_context* context() const { return ctx_; }
+
+    // One self-join of A over all diagonals > m/4, with the reference's log lines.
+    void join(const Scrimppp_params& params, const std::vector<double>& A, std::vector<double>& d2,
+              std::vector<int64_t>& idx) {
+        const int64_t n = (int64_t)A.size(), m = params.query_window_len;
         const int64_t PL = n - m + 1;
-        std::vector<double> d2(PL);
-        std::vector<int64_t> idx(PL);
+        d2.assign(PL, 0.0);
+        idx.assign(PL, 0);
         const auto t0 = std::chrono::steady_clock::now();
         const int rc = mp_selfjoin(ctx_, A.data(), n, m, -1, precision_, params.reanchor_k,
                                    params.block_length, 0, 0, d2.data(), idx.data(), nullptr);
@@ -94,11 +108,7 @@ public:
         std::clog << "throughput computations: " << tri * tri / sec << " matrix entries/second"
                   << std::endl;
         std::clog << "true cells/second: " << (tri - 1.0) * tri / 2.0 / sec << std::endl;
-        store_profile(params, d2, idx);
     }
-
-protected:
-    mp_context* context() const { return ctx_; }
 
 private:
     int precision_;
@@ -116,11 +126,13 @@ public:
 
 // SCRIMP++ (ScrimpppOrig::compute_matrix_profile, scrimppp/src/ScrimpppOrig.cpp:
 // 37-395): the PreSCRIMP approximate profile goes to "<output>_prescrimp"
-// (always ASCII, as the reference writes it, :268-279), then the exact
-// profile of all diagonals to <output>.  The exact phase is the FP64 form:
+// (always ASCII, as the reference writes it, :268-279), then the final
+// profile to <output>: the exact phase (the FP64 form over all diagonals > m/4,
 // the same values as scrimp_vert_blocked; the reference's own SCRIMP phase
-// forms distances with sqrt-variance arithmetic (:300-330) and agrees with
-// them to rounding.
+// forms distances with sqrt-variance arithmetic, :300-330, and agrees with them
+// to rounding) lowered by PreSCRIMP's neighbours exactly m/4 away, which the
+// reference keeps because its exact phase never reaches them
+// (merge_prescrimp_lag).
 class GpuScrimppp : public GpuVertBlocked {
 public:
     GpuScrimppp() : GpuVertBlocked(MP_PREC_FP64) {}
@@ -146,7 +158,11 @@ public:
         if (params.output_filename.empty())
             throw std::invalid_argument("Empty output file name specified!");
         io::write_profile_ascii(params.output_filename + "_prescrimp", d2.data(), idx.data(), PL);
-        GpuVertBlocked::compute_matrix_profile(params);
+        std::vector<double> xd2;
+        std::vector<int64_t> xidx;
+        join(params, A, xd2, xidx);
+        merge_prescrimp_lag(PL, m / 4, d2.data(), idx.data(), xd2.data(), xidx.data());
+        store_profile(params, xd2, xidx);
     }
 };
 
