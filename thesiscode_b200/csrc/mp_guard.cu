@@ -22,7 +22,6 @@ namespace mpgpu {
 
 namespace {
 
-constexpr double kGuardRatio = 16.0;
 constexpr unsigned long long kNoKey = ~0ull;
 
 __device__ __forceinline__ unsigned long long guard_key(float u, int64_t nb) {
@@ -141,20 +140,7 @@ __global__ void __launch_bounds__(128) fp64_guard_kernel(const Fp32TileParams* _
 // ignored by fmin).
 __global__ void hazard_block_minima_kernel(const double* __restrict__ nn, int64_t PL, int64_t blk,
                                            double* __restrict__ pre, double* __restrict__ suf) {
-    const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t i0 = b * blk;
-    if (i0 >= PL) return;
-    const int64_t i1 = min(i0 + blk, PL);
-    double v = __longlong_as_double(0x7ff8000000000000ll);
-    for (int64_t i = i0; i < i1; ++i) {
-        v = fmin(v, nn[i]);
-        pre[i] = v;
-    }
-    v = __longlong_as_double(0x7ff8000000000000ll);
-    for (int64_t i = i1 - 1; i >= i0; --i) {
-        v = fmin(v, nn[i]);
-        suf[i] = v;
-    }
+    hazard_block_minima(nn, PL, blk, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, pre, suf);
 }
 
 // Part 2: flag[w + 1] = 1 when window w is a hazard: flat, or its inverse norm
@@ -170,16 +156,7 @@ __global__ void hazard_flags_kernel(const double* __restrict__ nn, const double*
             flag[0] = 0;
             continue;
         }
-        const int64_t look = blk - 1;
-        double mn;
-        if (w < look) {
-            mn = pre[w];
-        } else {
-            const int64_t a = w - look;
-            mn = (a % blk == 0) ? pre[w] : fmin(suf[a], pre[w]);
-        }
-        const double x = nn[w];
-        flag[w + 1] = (x != x || x > kGuardRatio * mn) ? 1 : 0;
+        flag[w + 1] = hazard_flag(nn, pre, suf, blk, w);
     }
 }
 

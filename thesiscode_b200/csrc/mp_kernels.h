@@ -121,6 +121,46 @@ void launch_fp32_join(const Fp32TileParams* series_dev, int nseries, int64_t tot
 template <int R>
 void configure_fp32_join();
 // Guarded form (mp_guard.cu): hazard windows and the FP64 pass over their tiles.
+#ifdef __CUDACC__
+// The hazard rule, host-callable so that it can be checked without a GPU.
+// Window w is a hazard when it is flat (NaN inverse norm) or its inverse norm
+// exceeds kGuardRatio times the smallest inverse norm among windows
+// [w - (blk - 1), w]; that minimum comes from a van Herk / Gil-Werman sliding
+// minimum: prefix and suffix minima within blocks of blk windows (fmin ignores
+// NaN, so flat windows never lower it).
+constexpr double kGuardRatio = 16.0;
+// Block b: pre[i] = min nn[b*blk .. i], suf[i] = min nn[i .. end of block b].
+__host__ __device__ inline void hazard_block_minima(const double* nn, int64_t PL, int64_t blk,
+                                                    int64_t b, double* pre, double* suf) {
+    const int64_t i0 = b * blk;
+    if (i0 >= PL) return;
+    const int64_t i1 = i0 + blk < PL ? i0 + blk : PL;
+    double v = nn[i0];
+    for (int64_t i = i0; i < i1; ++i) {
+        v = fmin(v, nn[i]);
+        pre[i] = v;
+    }
+    v = nn[i1 - 1];
+    for (int64_t i = i1 - 1; i >= i0; --i) {
+        v = fmin(v, nn[i]);
+        suf[i] = v;
+    }
+}
+// 1 when window w (< PL) is a hazard, from the block minima above.
+__host__ __device__ inline int hazard_flag(const double* nn, const double* pre, const double* suf,
+                                           int64_t blk, int64_t w) {
+    const int64_t look = blk - 1;
+    double mn;
+    if (w < look) {
+        mn = pre[w];
+    } else {
+        const int64_t a = w - look;
+        mn = (a % blk == 0) ? pre[w] : fmin(suf[a], pre[w]);
+    }
+    const double x = nn[w];
+    return (x != x || x > kGuardRatio * mn) ? 1 : 0;
+}
+#endif
 __global__ void hazard_block_minima_kernel(const double* nn, int64_t PL, int64_t blk, double* pre,
                                            double* suf);
 __global__ void hazard_flags_kernel(const double* nn, const double* pre, const double* suf,
