@@ -15,7 +15,9 @@ records what those binaries output:
   edge_cases.npz     small seeded cases: tiny series, blocklen not a multiple
                      of 4, zero- and non-zero-level flat segments, n == m,
                      a single diagonal, odd m, a large offset
-  digests.json       sha256 of the reference's d2/idx bytes for workload c1
+  digests.json       sha256 of the reference's own binary copy of test.ascii
+                     (data_testing/test.bin, series format 2), and
+                     sha256 of the reference's d2/idx bytes for workload c1
                      (n = 65,536, m = 400), and with --big for c2
                      (n = 1,048,576, m = 256, values from the threaded triv_par
                      re-hosting; indices may only differ on exact ties)
@@ -118,6 +120,8 @@ def main():
     np.savez_compressed(os.path.join(HERE, "edge_cases.npz"), **ec)
 
     dig = {}
+    tb = open(os.path.join(REF_SRC, "data_testing", "test.bin"), "rb").read()
+    dig["test_bin"] = {"bytes": len(tb), "sha256": hashlib.sha256(tb).hexdigest()}
     x, m = workloads.c1()
     d2, idx, sec = ieee.vert_blocked(x, m, shuffle=True)
     dig["c1"] = {"n": int(x.size), "m": m, "d2_sha256": sha(d2), "idx_sha256": sha(idx),

@@ -184,3 +184,19 @@ def test_wrong_format_or_offset_is_an_error(driver, tmp_path):
     assert r.returncode == 1 and "unexpected data offset" in r.stderr
     r = _run(driver, "read_series_bin", str(tmp_path / "missing.bin"))
     assert r.returncode == 1 and "Could not open input file" in r.stderr
+
+
+def test_writer_reproduces_the_reference_binary_series_file(driver, tmp_path, golden_ascii, digests):
+    # the reference ships test.ascii and its binary copy test.bin (format 2);
+    # written from test.ascii's values, our file must be that file byte for byte
+    import hashlib
+    x = golden_ascii["series"]
+    g = tmp_path / "test.bin"
+    r = _run(driver, "write_series_bin", str(g), stdin=_stdin(x, np.zeros(x.size)))
+    assert r.returncode == 0, r.stderr
+    raw = g.read_bytes()
+    assert len(raw) == digests["test_bin"]["bytes"]
+    assert hashlib.sha256(raw).hexdigest() == digests["test_bin"]["sha256"]
+    r = _run(driver, "read_series_bin", str(g))
+    assert r.returncode == 0 and _values(r.stdout)[0] == x.size
+    assert np.array_equal(validate.read_series(str(g)), x)
