@@ -17,7 +17,8 @@ and 5 (the reference's stride is an integer multiple of the window), and the
 smallest series, where the FFT size is 2m instead of n
 (ScrimpppOrig.cpp:127-128), and slowly chirped sines of period m/4, whose
 nearest neighbours lie exactly m/4 away: PreSCRIMP accepts that lag, the exact
-diagonals start one further.  No flat windows: there the reference divides
+diagonals start one further; and the reference README's example
+(scrimppp_orig 400 100 on its own data_testing/test.ascii).  No flat windows: there the reference divides
 FFT rounding noise by a zero standard deviation, so its result depends on
 FFTW's exact rounding.
 """
@@ -34,7 +35,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from oracle.oracle import REF_DIR, build  # noqa: E402
+from oracle.oracle import REF_DIR, REF_SRC, build  # noqa: E402
 
 BINARY = os.path.join(REF_DIR, "scrimppp_ref_orig")
 
@@ -53,7 +54,15 @@ def cases():
         ("walk_n100_m64_s1", walk(100), 64, 1),
         ("chirp_n2048_m64_s1", chirp(2048, 64, 2e-6, 1e-3, rng), 64, 1),
         ("chirp_n2000_m40_s2", chirp(2000, 40, 1e-5, 1e-3, rng), 40, 2),
+        # the reference README's example, scrimppp_orig 400 100 on its test.ascii: one
+        # query, whose walk runs the whole length of its best diagonal
+        ("readme_test_ascii_m400_s100", test_ascii(), 400, 100),
     ]
+
+
+def test_ascii():
+    return np.array(open(os.path.join(REF_SRC, "data_testing", "test.ascii")).read().split(),
+                    dtype=np.float64)
 
 
 def chirp(n, m, alpha, eps, rng):

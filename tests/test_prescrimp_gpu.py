@@ -86,7 +86,8 @@ def test_cli_scrimppp_writes_prescrimp_and_exact_profiles(tmp_path, golden_ascii
     assert os.path.getsize(str(out) + "_prescrimp") > 0
 
 
-@pytest.mark.parametrize("case", ["chirp_n2048_m64_s1", "walk_n1500_m50_s1"])
+@pytest.mark.parametrize("case", ["chirp_n2048_m64_s1", "walk_n1500_m50_s1",
+                                  "readme_test_ascii_m400_s100"])
 def test_cli_scrimppp_final_profile_is_the_reference(tmp_path, golden_prescrimp, case):
     # gpu_scrimppp's two files against the reference scrimppp_orig's; on the
     # chirped sine hundreds of neighbours lie exactly m/4 away, where only
