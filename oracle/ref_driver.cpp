@@ -213,14 +213,14 @@ int ref_triv_par_threads(const double* A, long n, long m, long blocklen, long di
 }  // extern "C"
 
 /* Command line: <algo> <window-length> <prescrimp-stride> <input-file>
- *               [--blocklen B] [--output-file F]
+ *               [--blocklen B] [--output-file F] [--filetype ASCII|BIN]
  * Runs the reference's factory + compute_matrix_profile on an ASCII series,
  * the same calls its main() makes (scrimppp/src/main.cpp:47-80). */
 int main(int argc, char** argv) {
     if (argc < 5) {
         std::fprintf(stderr,
                      "usage: %s <algo> <window-length> <prescrimp-stride> <input-file> "
-                     "[--blocklen B] [--output-file F]\navailable: %s\n",
+                     "[--blocklen B] [--output-file F] [--filetype ASCII|BIN]\navailable: %s\n",
                      argv[0], MatProfImplFactory::getInstance().get_available_implementations().c_str());
         return 2;
     }
@@ -234,6 +234,9 @@ int main(int argc, char** argv) {
     for (int i = 5; i + 1 < argc; i += 2) {
         std::string k = argv[i];
         if (k == "--blocklen") p.block_length = std::atoi(argv[i + 1]);
+        else if (k == "--filetype")  // BIN needs the reference's MPI-IO classes (scrimppp_ref_bin)
+            p.filetype = std::string(argv[i + 1]) == "BIN" ? Scrimppp_params::BIN
+                                                          : Scrimppp_params::ASCII;
         else if (k == "--output-file") p.output_filename = argv[i + 1];
     }
     if (p.output_filename.empty()) {

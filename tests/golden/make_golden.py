@@ -16,7 +16,10 @@ records what those binaries output:
                      of 4, zero- and non-zero-level flat segments, n == m,
                      a single diagonal, odd m, a large offset
   digests.json       sha256 of the reference's own binary copy of test.ascii
-                     (data_testing/test.bin, series format 2), and
+                     (data_testing/test.bin, series format 2); of the binary
+                     profile (format 1) the reference's MPI-IO classes write
+                     for test.bin with m = 64 (oracle/_ref/scrimppp_ref_bin,
+                     --filetype BIN); and
                      sha256 of the reference's d2/idx bytes for workload c1
                      (n = 65,536, m = 400), and with --big for c2
                      (n = 1,048,576, m = 256, values from the threaded triv_par
@@ -122,6 +125,16 @@ def main():
     dig = {}
     tb = open(os.path.join(REF_SRC, "data_testing", "test.bin"), "rb").read()
     dig["test_bin"] = {"bytes": len(tb), "sha256": hashlib.sha256(tb).hexdigest()}
+    with tempfile.TemporaryDirectory() as td:
+        of = os.path.join(td, "prof.bin")
+        subprocess.run([os.path.join(ROOT, "oracle", "_ref", "scrimppp_ref_bin"),
+                        "scrimp_vert_blocked", "64", "1",
+                        os.path.join(REF_SRC, "data_testing", "test.bin"),
+                        "--filetype", "BIN", "--output-file", of], check=True, capture_output=True)
+        pb = open(of, "rb").read()
+    rec = np.frombuffer(pb[100:], dtype=[("d2", "<f8"), ("idx", "<u8")])
+    assert np.array_equal(rec["d2"], out["d2_m64"])  # the binary read gave the same series
+    dig["bin_profile_test_bin_m64"] = {"bytes": len(pb), "sha256": hashlib.sha256(pb).hexdigest()}
     x, m = workloads.c1()
     d2, idx, sec = ieee.vert_blocked(x, m, shuffle=True)
     dig["c1"] = {"n": int(x.size), "m": m, "d2_sha256": sha(d2), "idx_sha256": sha(idx),

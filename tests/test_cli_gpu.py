@@ -45,7 +45,7 @@ def test_cli_default_output_name(tmp_path, golden_ascii):
     assert (tmp_path / "gpu_vert_blocked_fp32k_new_MatrixProfile_64series.ascii.matprof.ascii").exists()
 
 
-def test_cli_binary_round_trip(tmp_path, golden_ascii):
+def test_cli_binary_round_trip(tmp_path, golden_ascii, digests):
     x = golden_ascii["series"]
     hdr = np.zeros(100, dtype=np.uint8)
     hdr[:16] = np.frombuffer(np.array([2, 100], dtype="<u4").tobytes()
@@ -63,6 +63,10 @@ def test_cli_binary_round_trip(tmp_path, golden_ascii):
     rec = np.frombuffer(b[100:], dtype=[("d2", "<f8"), ("idx", "<u8")])
     assert np.array_equal(rec["d2"], golden_ascii["d2_m64"])  # binary stores d2, not sqrt
     assert np.array_equal(rec["idx"].astype(np.int64), golden_ascii["idx_m64"])
+    # the input is the reference's test.bin and the output the file its own MPI-IO
+    # writer makes for it, byte for byte
+    assert hashlib.sha256(inp.read_bytes()).hexdigest() == digests["test_bin"]["sha256"]
+    assert hashlib.sha256(b).hexdigest() == digests["bin_profile_test_bin_m64"]["sha256"]
 
 
 def test_run_algorithm_through_registry(tmp_path, golden_ascii):

@@ -200,3 +200,40 @@ def test_writer_reproduces_the_reference_binary_series_file(driver, tmp_path, go
     r = _run(driver, "read_series_bin", str(g))
     assert r.returncode == 0 and _values(r.stdout)[0] == x.size
     assert np.array_equal(validate.read_series(str(g)), x)
+
+
+def test_writer_reproduces_the_reference_binary_profile_file(driver, tmp_path, golden_ascii, digests):
+    # the reference's MPI-IO profile writer (binproffile.cpp, run for its test.bin with
+    # m = 64) made a file with this digest; ours, given the same profile, must match
+    import hashlib
+    d2, idx = golden_ascii["d2_m64"], golden_ascii["idx_m64"]
+    g = tmp_path / "prof.bin"
+    r = _run(driver, "write_profile_bin", str(g), stdin=_stdin(d2, idx))
+    assert r.returncode == 0, r.stderr
+    raw = g.read_bytes()
+    assert len(raw) == digests["bin_profile_test_bin_m64"]["bytes"]
+    assert hashlib.sha256(raw).hexdigest() == digests["bin_profile_test_bin_m64"]["sha256"]
+
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "scrimppp_ref_bin")),
+                    reason="oracle/_ref not built (no reference tree)")
+def test_files_interchange_with_the_reference(driver, tmp_path, oracle):
+    # our series file goes into the reference's binary reader; the reference's binary
+    # profile comes back through our reader
+    from thesiscode_b200 import workloads
+    x, m = workloads.random_walk(1500, 11), 40
+    s = tmp_path / "series.bin"
+    r = _run(driver, "write_series_bin", str(s), stdin=_stdin(x, np.zeros(x.size)))
+    assert r.returncode == 0, r.stderr
+    p = tmp_path / "prof.bin"
+    ref = os.path.join(ROOT, "oracle", "_ref", "scrimppp_ref_bin")
+    subprocess.run([ref, "scrimp_vert_blocked", str(m), "1", str(s), "--filetype", "BIN",
+                    "--output-file", str(p)], check=True, capture_output=True)
+    r = _run(driver, "read_profile_bin", str(p))
+    assert r.returncode == 0, r.stderr
+    n, rows = _values(r.stdout)
+    d2, idx = oracle.selfjoin(x, m)
+    assert n == d2.size
+    assert np.array_equal(np.array([float(v[0]) for v in rows]), d2)
+    assert np.array_equal(np.array([int(v[1]) for v in rows]), idx)
