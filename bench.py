@@ -111,6 +111,12 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+SERIES_KIND = {
+    "c3": "random walk with 32 sine motifs and 16 constant stretches at the walk's level,",
+    "c3z": "random walk with 32 sine motifs and 16 constant stretches at level 0,",
+}
+
+
 def read_ncu_traffic(kernel: str):
     """dram bytes per launch recorded in profiles/ (from one ncu capture)."""
     path = os.path.join(ROOT, "profiles", f"{kernel}.txt")
@@ -189,6 +195,9 @@ def run_ours(args, world):
     dev = torch.device("cuda", local)
     if args.workload == "c1":
         x, m = wl.c1()
+    elif args.workload in ("c3", "c3z"):
+        # long stress series: motifs and constant stretches (at the walk's level, or 0)
+        x, m, _ = wl.c3(zero_level=args.workload == "c3z")
     else:
         x, m = wl.c2()
     n = x.size
@@ -373,7 +382,7 @@ def run_ours(args, world):
         except Exception:
             peaks[name] = None
     peak32 = max(v for v in (peaks["f32_ffma"], peaks["f32x2_ffma2"]) if v)
-    traffic = read_ncu_traffic("fp32_join_kernel_c2")
+    traffic = read_ncu_traffic(f"fp32_join_kernel_{args.workload}")  # null without a capture
     roofline = {
         "bound": "fp32-fma-pipe (CUDA cores; no tensor-core or HBM bound)",
         "achieved": achieved, "peak": peak32, "unit": "TFLOP/s", "frac": achieved / peak32,
@@ -393,11 +402,13 @@ def run_ours(args, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"{args.workload}: random walk n={n:,}, m={m}, excl={excl}, all "
+        "config": {"workload": f"{args.workload}: {SERIES_KIND.get(args.workload, 'random walk')} "
+                               f"n={n:,}, m={m}, excl={excl}, all "
                                f"diagonals; FP32 recurrence re-anchored in FP64 every "
                                f"K={args.reanchor_k} steps",
                    "n": n, "m": m, "reanchor_k": args.reanchor_k, "cells": cells_total,
-                   "l2": "flushed between steps (256 MB write); working set ~100 MB",
+                   "l2": f"flushed between steps (256 MB write); working set "
+                         f"~{(8 * n + 80 * PL) / 1e6:.0f} MB",
                    "parallelism": f"diagonal partitions x{2 * world}, NCCL all-gather merge"
                    if world > 1 else "single GPU"},
         "fp64_baseline": {"value": value64, "unit": "cells/s", "ms_per_step": tot64 / fsteps,
@@ -537,7 +548,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["c2", "c1", "c4", "c5"], default="c2")
+    ap.add_argument("--workload", choices=["c2", "c1", "c3", "c3z", "c4", "c5"], default="c2")
     ap.add_argument("--c4-count", type=int, default=4096)
     ap.add_argument("--rates", type=float, nargs="+", default=[10, 30, 100, 300])
     ap.add_argument("--serve-seconds", type=float, default=10.0)
