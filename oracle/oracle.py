@@ -7,6 +7,12 @@ ctypes front end for
     compiled unchanged (oracle/Makefile), present where the reference tree was
     available at build time.
 
+The same recipe builds command-line programs of the reference, run as
+subprocesses by the tests and the golden-fixture scripts: ``scrimppp_ref_ieee``
+and ``scrimppp_ref_fast`` (its CLI), ``scrimppp_ref_orig`` (plus SCRIMP++ over
+a stand-in FFT) and ``scrimppp_ref_bin`` (plus its binary MPI-IO file classes
+over a single-rank emulation).
+
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import
 this module, and only to check or time the reference algorithm on the host.
 """
