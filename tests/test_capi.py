@@ -136,3 +136,20 @@ def test_allocation_free_entry_checks_arguments_before_the_device():
     assert rc == mp.MP_ERR_INVALID_ARG and b"shorter" in err.value
     rc = L.mp_selfjoin_fp32_noalloc(fake, 1 << 20, 10, -1, 0, fake, fake, None, err, 256)
     assert rc == mp.MP_ERR_NOT_SUPPORTED and b"mp_selfjoin" in err.value
+
+
+def test_cli_accepts_the_reference_options(tmp_path):
+    # --dbg (waits for Enter), --dist-io and --chunksize are the reference CLI's; they parse
+    # here, and the run then stops only for want of a B200 (or succeeds on one)
+    import torch
+    x = tmp_path / "x.ascii"
+    x.write_text(" ".join(str(float(v)) for v in range(300)))
+    r = subprocess.run([mp.CLI_PATH, "gpu_vert_blocked_fp64", "32", "8", str(x), "--dist-io", "false",
+                        "--chunksize", "100", "--dbg", "--output-file", str(tmp_path / "o.ascii")],
+                       input="\n", capture_output=True, text=True, timeout=120)
+    assert "parsing" not in r.stderr and "Press ENTER" in r.stdout
+    if not torch.cuda.is_available():
+        assert r.returncode == 1 and "no usable device" in r.stderr
+    r = subprocess.run([mp.CLI_PATH, "gpu_vert_blocked_fp64", "32", "8", str(x), "--dist-io", "maybe"],
+                       capture_output=True, text=True)
+    assert r.returncode != 0 and "invalid boolean" in r.stderr

@@ -1,7 +1,11 @@
 // Command line with the reference's interface (scrimppp/src/main.cpp:176-278):
 //   mpgpu_cli <algo> <window-length> <prescrimp-stride> <input-file>
 //             [--blocklen B] [--output-file F] [--filetype BIN|ASCII|BY_SUFFIX]
-//             [--reanchor-k K] [--device D]
+//             [--reanchor-k K] [--device D] [--dbg] [--dist-io BOOL] [--chunksize C]
+// --dbg waits for Enter before computing (a chance to attach a debugger), as in
+// the reference; --dist-io and --chunksize choose how the reference's MPI ranks
+// share binary file I/O: a single process writes the same bytes either way, so
+// they are recorded in the parameters and change nothing here.
 // The four positional arguments may also be given as --algo, --window-length,
 // --prescrimp-stride, --input-file.  The file type follows the input suffix
 // (.bin / .ascii) unless given; the default output name is
@@ -18,10 +22,17 @@
 
 using namespace matrix_profile;
 
+// Boolean option values as the reference's option parser takes them.
+static bool parse_bool(const std::string& v) {
+    if (v == "1" || v == "true" || v == "yes" || v == "on") return true;
+    if (v == "0" || v == "false" || v == "no" || v == "off") return false;
+    throw std::invalid_argument("invalid boolean " + v);
+}
+
 static void usage() {
     std::cout << "usage: mpgpu_cli <algo> <window-length> <prescrimp-stride> <input-file>\n"
                  "       [--blocklen B] [--output-file F] [--filetype BIN|ASCII|BY_SUFFIX]\n"
-                 "       [--reanchor-k K] [--device D]\n"
+                 "       [--reanchor-k K] [--device D] [--dbg] [--dist-io BOOL] [--chunksize C]\n"
                  "algorithms: "
               << MatProfImplFactory::getInstance().get_available_implementations() << "\n";
 }
@@ -30,6 +41,7 @@ int main(int argc, char** argv) {
     Scrimppp_params p;
     p.output_filename = "";
     std::vector<std::string> pos;
+    bool wait_debugger = false;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
         auto val = [&](const char* name) -> std::string {
@@ -48,6 +60,9 @@ int main(int argc, char** argv) {
             else if (a == "--output-file") p.output_filename = val("--output-file");
             else if (a == "--reanchor-k") p.reanchor_k = std::stol(val("--reanchor-k"));
             else if (a == "--device") p.device = std::stoi(val("--device"));
+            else if (a == "--dbg") wait_debugger = true;
+            else if (a == "--dist-io") p.use_distributed_io = parse_bool(val("--dist-io"));
+            else if (a == "--chunksize") p.writing_chunk_size = std::stoi(val("--chunksize"));
             else if (a == "--filetype") {
                 const std::string t = val("--filetype");
                 if (t == "BIN") p.filetype = Scrimppp_params::BIN;
@@ -89,6 +104,13 @@ int main(int argc, char** argv) {
         if (k != std::string::npos) base = base.substr(k + 1);
         p.output_filename = p.algo_name + "_new_MatrixProfile_" + std::to_string(p.query_window_len) +
                             base + ".matprof" + (p.filetype == Scrimppp_params::BIN ? ".bin" : ".ascii");
+    }
+    if (wait_debugger) {  // scrimppp/src/main.cpp:271-276
+        std::cout << "Waiting for user input before proceeding. Chance to attach a debugger..."
+                  << std::endl
+                  << "Press ENTER to continue...";
+        std::cout.flush();
+        std::cin.get();
     }
     std::unique_ptr<IMatProfAlgo> algo;
     try {
