@@ -153,3 +153,47 @@ def test_cli_accepts_the_reference_options(tmp_path):
     r = subprocess.run([mp.CLI_PATH, "gpu_vert_blocked_fp64", "32", "8", str(x), "--dist-io", "maybe"],
                        capture_output=True, text=True)
     assert r.returncode != 0 and "invalid boolean" in r.stderr
+
+
+C_PROGRAM = r"""
+#include <stdio.h>
+#include <string.h>
+#include "mpgpu.h"
+
+int main(void) {
+    mp_context* ctx = NULL;
+    char names[256];
+    int need = mp_list_algorithms(names, sizeof names);
+    if (need <= 1 || strstr(names, "gpu_vert_blocked_fp64") == NULL) return 10;
+    if (strcmp(mp_status_string(MP_OK), "ok") != 0) return 11;
+    if (mp_selfjoin_scratch_bytes(1 << 16, 256, MP_PREC_FP32_REANCHOR) == 0) return 12;
+    if (mp_selfjoin(NULL, NULL, 0, 0, -1, MP_PREC_FP64, 0, 0, 0, 0, NULL, NULL, NULL)
+        != MP_ERR_INVALID_ARG) return 13;
+    {
+        const int rc = mp_context_create(0, 0, &ctx);
+        printf("%d\n", rc);
+        if (rc == MP_OK) mp_context_destroy(ctx);
+        else if (rc != MP_ERR_NO_DEVICE) return 14;
+    }
+    return 0;
+}
+"""
+
+
+def test_header_compiles_as_c_and_links(tmp_path):
+    # the boundary is plain C: a C99 program includes mpgpu.h and links the library
+    import shutil
+    import torch
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    src = tmp_path / "use.c"
+    src.write_text(C_PROGRAM)
+    exe = tmp_path / "use"
+    libdir = os.path.dirname(mp.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", f"-I{os.path.join(ROOT, 'include')}",
+                    str(src), "-o", str(exe), f"-L{libdir}", "-lmpgpu", f"-Wl,-rpath,{libdir}"],
+                   check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    if not torch.cuda.is_available():
+        assert r.stdout.strip() == str(mp.MP_ERR_NO_DEVICE)
