@@ -26,7 +26,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
-REF_SRC = os.environ.get("SCRIMP_REF_ROOT", "/root/reference/scrimppp")
+# The reference's scrimppp directory (sources, data_testing/).  Needed only to
+# build oracle/_ref or to regenerate the golden fixtures; unset means absent.
+REF_SRC = os.environ.get("SCRIMP_REF_ROOT", "")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _L = ctypes.POINTER(ctypes.c_int64)
@@ -37,7 +39,10 @@ def build(with_reference: bool | None = None) -> None:
     """Compile the C restatement, and the reference-source oracle when the
     reference tree is present (or ``with_reference`` forces it)."""
     targets = ["oracle"]
-    if with_reference or (with_reference is None and os.path.isdir(REF_SRC)):
+    if with_reference and not REF_SRC:
+        raise RuntimeError("oracle.build(with_reference=True) needs SCRIMP_REF_ROOT: the "
+                           "reference's scrimppp directory")
+    if with_reference or (with_reference is None and REF_SRC and os.path.isdir(REF_SRC)):
         targets.append("ref")
     subprocess.run(["make", "-s", "-C", HERE, f"REF={REF_SRC}", *targets], check=True)
 

@@ -1,7 +1,8 @@
 """Regenerates the golden fixtures in this directory from the REFERENCE itself.
 
 Run in a container where the reference tree exists (it is read at build time
-only): ``python tests/golden/make_golden.py [--big]``.  It builds
+only): ``SCRIMP_REF_ROOT=<reference checkout>/scrimppp python
+tests/golden/make_golden.py [--big]``.  It builds
 oracle/_ref from the reference's unchanged sources (oracle/Makefile) and
 records what those binaries output:
 

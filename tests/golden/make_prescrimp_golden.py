@@ -1,6 +1,7 @@
 """Regenerates tests/golden/prescrimp_ref.npz from the REFERENCE's PreSCRIMP.
 
-Run where the reference tree exists: ``python tests/golden/make_prescrimp_golden.py``.
+Run where the reference tree exists: ``SCRIMP_REF_ROOT=<reference checkout>/scrimppp
+python tests/golden/make_prescrimp_golden.py``.
 It builds oracle/_ref/scrimppp_ref_orig (oracle/Makefile: the reference's
 ScrimpppOrig.cpp and the hot-path sources, unchanged, IEEE build, with the
 stand-in FFT of oracle/ref_fftw_stub.cpp in place of FFTW), runs the
