@@ -88,11 +88,36 @@ def test_autotune_lookup(tmp_path, monkeypatch):
     assert autotune.lookup(3_000, 1024) == 1024  # not in the table: the default
     monkeypatch.setenv("MPGPU_AUTOTUNE_TABLE", str(tmp_path / "missing.json"))
     assert autotune.lookup(20_000, 128) == 1024
+    # entries with their measured error (the current format)
+    table2 = tmp_path / "t2.json"
+    table2.write_text(json.dumps({"_bound": 1e-4, "128:14": {"K": 512, "max_rel_err": 3e-5,
+                                                             "join_ms": 1.0,
+                                                             "within_bound": True}}))
+    monkeypatch.setenv("MPGPU_AUTOTUNE_TABLE", str(table2))
+    assert autotune.lookup(20_000, 128) == 512
+
+
+def test_autotune_choice_is_gated_on_error():
+    # the fastest candidate whose measured error is within the bound (with margin)
+    trials = [(1024, 1.0, 1.2e-4), (512, 1.5, 7e-5), (256, 2.0, 5e-5), (128, 3.0, 4e-5)]
+    e = autotune.choose(trials)
+    assert e["K"] == 512 and e["within_bound"] and e["max_rel_err"] == 7e-5
+    # nothing within the bound: the most accurate one, flagged
+    e = autotune.choose([(1024, 1.0, 3e-4), (256, 2.0, 1.5e-4)])
+    assert e["K"] == 256 and not e["within_bound"]
+    # margin: 9e-5 is inside 1e-4 but not inside 0.8e-4
+    assert autotune.choose([(1024, 1.0, 9e-5), (128, 4.0, 1e-5)])["K"] == 128
 
 
 def test_committed_autotune_table_is_complete():
     t = json.load(open(autotune.DEFAULT_TABLE))
-    for key, K in t.items():
+    for key, e in t.items():
+        if key.startswith("_"):
+            continue
         m, b = key.split(":")
         assert int(m) in autotune.WINDOWS and int(b) in autotune.BUCKETS
+        K = e["K"] if isinstance(e, dict) else e
         assert K in autotune.CANDIDATES
+        if isinstance(e, dict):
+            # an entry is within the bound, or the most accurate candidate was kept
+            assert e["within_bound"] == (e["max_rel_err"] <= autotune.SAFETY * autotune.ERROR_BOUND)
