@@ -90,6 +90,8 @@ size_t mp_selfjoin_scratch_bytes(int64_t n, int64_t m, int precision);
  *   idx_out      PL int64 neighbour indices (host or device).
  *   stream       cudaStream_t (NULL = legacy default stream).
  * The call returns after the results are written (it synchronises stream).
+ * Device buffers must belong to the context's device: device memory of
+ * another GPU returns MP_ERR_INVALID_ARG before anything is launched.
  */
 int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t excl,
                 int precision, int64_t reanchor_k, int64_t blocklen, int64_t diag_lo,
@@ -215,7 +217,10 @@ int mp_server_destroy(mp_server* s);
  *
  * The first call on a device (the current device at the time of the call)
  * looks up the scratch's device address and configures the join kernel
- * there; make that first call before any stream capture.  All calls on a
+ * there; make that first call before any stream capture.  Both are kept for
+ * the life of the process, so resetting that device (cudaDeviceReset) after
+ * the first call is not supported.  Buffers on another GPU are refused with
+ * MP_ERR_INVALID_ARG before anything is launched.  All calls on a
  * device share the one scratch array: calls whose work overlaps on the GPU
  * (other streams, other host threads) race and corrupt each other's results,
  * so serialise them (one stream, or events between streams).

@@ -42,18 +42,27 @@ def _series(seed, n):
     return x
 
 
-def _noalloc(f, torch, x, m, k):
+def _buffers(torch, x, m):
     A = torch.from_numpy(x).cuda()
     PL = x.size - m + 1
     d2 = torch.full((PL,), -1.0, dtype=torch.float64, device="cuda")
     ix = torch.full((PL,), -1, dtype=torch.int64, device="cuda")
     torch.cuda.synchronize()
+    return A, d2, ix
+
+
+def _call(f, torch, bufs, n, m, k, excl=-1):
+    A, d2, ix = bufs
     err = ctypes.create_string_buffer(256)
-    rc = f(A.data_ptr(), x.size, m, -1, k, d2.data_ptr(), ix.data_ptr(),
+    rc = f(A.data_ptr(), n, m, excl, k, d2.data_ptr(), ix.data_ptr(),
            torch.cuda.current_stream().cuda_stream, err, len(err))
     assert rc == 0, err.value.decode()
     torch.cuda.synchronize()
     return d2.cpu().numpy(), ix.cpu().numpy()
+
+
+def _noalloc(f, torch, x, m, k, excl=-1):
+    return _call(f, torch, _buffers(torch, x, m), x.size, m, k, excl)
 
 
 def _check_same(got, want):
@@ -85,3 +94,50 @@ def test_noalloc_rejects_series_beyond_limit():
            len(err))
     assert rc == MP_ERR_NOT_SUPPORTED
     assert b"allocation-free limit" in err.value
+
+
+def test_noalloc_allocates_nothing(gpu_ctx):
+    """After a first call (which only looks up the scratch address), further
+    calls leave the device's free memory and torch's allocator untouched."""
+    import torch
+    f = _entry()
+    x, m, k = _series(13, 50_000), 128, 1024
+    bufs = _buffers(torch, x, m)
+    first = _call(f, torch, bufs, x.size, m, k)
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0 = torch.cuda.memory_allocated()
+    again = [_call(f, torch, bufs, x.size, m, k) for _ in range(2)]
+    free1, _ = torch.cuda.mem_get_info()
+    assert torch.cuda.memory_allocated() == alloc0
+    assert free1 == free0
+    for d2, ix in again:
+        assert np.array_equal(d2, first[0]) and np.array_equal(ix, first[1])
+
+
+@pytest.mark.parametrize("excl", [20, 9000])
+def test_noalloc_explicit_exclusion_zone(gpu_ctx, excl):
+    """An explicit exclusion zone, and one at least as long as the profile (no
+    diagonal is evaluated, so every window keeps the no-neighbour result)."""
+    import torch
+    f = _entry()
+    x, m, k = _series(14, 9000), 64, 256
+    want = gpu_ctx.selfjoin(x, m, precision=mp.FP32_REANCHOR, reanchor_k=k, excl=excl)
+    _check_same(_noalloc(f, torch, x, m, k, excl=excl), want)
+    if excl >= x.size - m + 1:
+        assert np.all(want.dist2 == 2 * m + 2)
+
+
+def test_noalloc_refuses_buffers_of_another_gpu():
+    """A buffer on another GPU is refused before anything is launched."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    f = _entry()
+    other = torch.zeros(4096, dtype=torch.float64, device="cuda:1")
+    mine = torch.zeros(4096, dtype=torch.float64, device="cuda:0")
+    torch.cuda.set_device(0)
+    err = ctypes.create_string_buffer(256)
+    rc = f(other.data_ptr(), 4096, 64, -1, 0, mine.data_ptr(), mine.data_ptr(), None, err,
+           len(err))
+    assert rc == mp.MP_ERR_INVALID_ARG
+    assert b"current device" in err.value

@@ -314,9 +314,15 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
     cudaStream_t st = (cudaStream_t)stream;
     ctx->launches = 0;
     ctx->near_duplicates = -1;
-    const bool a_dev = on_device(A);
-    const bool o_dev = on_device(dist2_out);
-    if (on_device(idx_out) != o_dev)
+    const MemSpace sa = mem_space(A, ctx->device), sd = mem_space(dist2_out, ctx->device),
+                   si = mem_space(idx_out, ctx->device);
+    if (sa == MemSpace::OtherDevice || sd == MemSpace::OtherDevice || si == MemSpace::OtherDevice)
+        return fail(ctx, MP_ERR_INVALID_ARG,
+                    "A, dist2_out and idx_out must be host memory or device memory of the "
+                    "context's device %d", ctx->device);
+    const bool a_dev = sa == MemSpace::Device;
+    const bool o_dev = sd == MemSpace::Device;
+    if ((si == MemSpace::Device) != o_dev)
         return fail(ctx, MP_ERR_INVALID_ARG, "dist2_out and idx_out live in different memory spaces");
     const int64_t PL = S.PL, ndiag = S.hi - S.lo;
 
@@ -593,8 +599,13 @@ int mp_prescrimp(mp_context* ctx, const double* A, int64_t n, int64_t m, double 
     ctx->launches = 0;
     const int64_t step = (int64_t)stepf;
     const int64_t Q = (PL + step - 1) / step;
-    const bool o_dev = on_device(dist2_out);
-    if (on_device(idx_out) != o_dev)
+    const MemSpace sd = mem_space(dist2_out, ctx->device), si = mem_space(idx_out, ctx->device);
+    if (sd == MemSpace::OtherDevice || si == MemSpace::OtherDevice)
+        return fail(ctx, MP_ERR_INVALID_ARG,
+                    "dist2_out and idx_out must be host memory or device memory of the "
+                    "context's device %d", ctx->device);
+    const bool o_dev = sd == MemSpace::Device;
+    if ((si == MemSpace::Device) != o_dev)
         return fail(ctx, MP_ERR_INVALID_ARG, "dist2_out and idx_out live in different memory spaces");
     size_t bytes = align_up(8 * (size_t)n) * 3 + align_up(8 * (size_t)PL) * 4 +
                    align_up(8 * (size_t)Q) * 2 + 4096;

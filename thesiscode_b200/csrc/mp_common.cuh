@@ -30,14 +30,22 @@ inline unsigned host_ord_f32(float v) {
 // Sub-buffers of a scratch arena start on 256-byte boundaries.
 constexpr size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
-// True for device (or managed) memory, false for host memory.
-inline bool on_device(const void* p) {
+// Where a caller's buffer lives, seen from device `device`: host memory
+// (pageable or pinned), memory the kernels on `device` may address (its own
+// device memory, or managed memory), or device memory of another GPU, which
+// the entry points refuse: a kernel on `device` would need peer access to
+// touch it, and without that the access faults.
+enum class MemSpace { Host, Device, OtherDevice };
+inline MemSpace mem_space(const void* p, int device) {
     cudaPointerAttributes at;
     if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
         cudaGetLastError();
-        return false;
+        return MemSpace::Host;
     }
-    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+    if (at.type == cudaMemoryTypeManaged) return MemSpace::Device;
+    if (at.type == cudaMemoryTypeDevice)
+        return at.device == device ? MemSpace::Device : MemSpace::OtherDevice;
+    return MemSpace::Host;
 }
 
 // Streaming multiprocessors of the current device (148 on a B200), read once

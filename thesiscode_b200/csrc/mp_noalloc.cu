@@ -76,7 +76,9 @@ int report(char* err, size_t len, int status, const char* fmt, ...) {
 
 // Device address of the scratch on the current device; the first call on a
 // device looks it up (and sets the join kernel's shared-memory limit there).
-int setup_current_device(void** out, char* err, size_t len) {
+// Both are kept for the life of the process: after a cudaDeviceReset of that
+// device they are stale, so a reset is not supported once a call has run.
+int setup_current_device(void** out, int* dev_out, char* err, size_t len) {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
         cudaGetLastError();
@@ -105,6 +107,7 @@ int setup_current_device(void** out, char* err, size_t len) {
         g_scratch_addr[dev] = p;
     }
     *out = g_scratch_addr[dev];
+    *dev_out = dev;
     return MP_OK;
 }
 
@@ -136,11 +139,13 @@ extern "C" int mp_selfjoin_fp32_noalloc(const double* A_dev, int64_t n, int64_t 
                       "(use mp_selfjoin for longer series)",
                       (long long)n, (long long)kMaxN);
     void* base = nullptr;
-    int rc = setup_current_device(&base, err, err_len);
+    int dev = -1;
+    int rc = setup_current_device(&base, &dev, err, err_len);
     if (rc != MP_OK) return rc;
-    if (!on_device(A_dev) || !on_device(dist2_dev) || !on_device(idx_dev))
+    if (mem_space(A_dev, dev) != MemSpace::Device || mem_space(dist2_dev, dev) != MemSpace::Device ||
+        mem_space(idx_dev, dev) != MemSpace::Device)
         return report(err, err_len, MP_ERR_INVALID_ARG,
-                      "A, dist2 and idx must be device memory of the current device");
+                      "A, dist2 and idx must be device memory of the current device %d", dev);
 
     cudaStream_t st = (cudaStream_t)stream;
     const Layout L = layout_for(n);
