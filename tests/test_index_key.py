@@ -109,3 +109,70 @@ def test_index_key_orders_and_decodes(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "0 failed" in r.stdout
+
+
+THRESHOLD_PROGRAM = r"""
+#include <cstdio>
+#include <random>
+#include "mp_common.cuh"
+#include "mp_kernels.h"
+using namespace mpgpu;
+
+static int fails = 0;
+#define CHECK(c, ...) do { if (!(c)) { if (fails++ < 10) { std::printf(__VA_ARGS__); std::printf("\n"); } } } while (0)
+
+int main() {
+    std::mt19937_64 rng(777);
+    std::uniform_real_distribution<double> U(0.0, 1.0);
+    long long checked = 0;
+    for (int64_t m : {4LL, 64LL, 256LL, 1024LL, 8192LL}) {
+        const long long vlo = key_vlo_bits(m);
+        for (int idx_bits : {bits_for(100), bits_for(1 << 20), bits_for((1 << 24) - 1),
+                             bits_for((1ull << 31) - 1)}) {
+            const double eps = fp64_threshold_eps(idx_bits), tiny = fp64_threshold_tiny((double)m);
+            const int mant = 57 - idx_bits;
+            for (int it = 0; it < 200000; ++it) {
+                // a merged score c (correlation in (-1/m, 1], some near 1) and a
+                // candidate x whose v lies within a few key quanta of c's
+                const int e = -(int)(rng() % 45);
+                double vc = std::ldexp(0.5 + U(rng), e) * (double)m;
+                if (rng() % 16 == 0) vc = -vc * 1e-3;  // score above m (rounding)
+                const double sc = (double)m - vc;
+                const double q = std::ldexp(std::fabs(vc), -mant);
+                const double vx = vc + (U(rng) * 6.0 - 3.0) * q;
+                const double sx = (double)m - vx;
+                const unsigned long long kc = idx_key_f64(sc, (double)m, 0, idx_bits, vlo) >> idx_bits;
+                const unsigned long long kx = idx_key_f64(sx, (double)m, 0, idx_bits, vlo) >> idx_bits;
+                const double t = fp64_threshold_below(sc, (double)m, eps, tiny);
+                CHECK(t < sc, "threshold not below the score: m=%lld s=%.17g t=%.17g",
+                      (long long)m, sc, t);
+                if (kx >= kc) {
+                    ++checked;
+                    CHECK(sx > t, "pruned a tying key: m=%lld bits=%d sc=%.17g sx=%.17g t=%.17g",
+                          (long long)m, idx_bits, sc, sx, t);
+                }
+            }
+        }
+    }
+    std::printf("%lld tying candidates, %d failed\n", checked, fails);
+    return fails ? 1 : 0;
+}
+"""
+
+
+def test_fp64_threshold_keeps_every_tying_key(tmp_path):
+    """The FP64 join skips the selection of a cell whose score does not exceed
+    its entry's threshold.  Thresholds sit below a merged score by more than the
+    index key resolves, so a candidate whose key could still tie or beat that
+    score's key always exceeds them: skipping cannot change either key."""
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not available")
+    src = tmp_path / "thr.cu"
+    src.write_text(THRESHOLD_PROGRAM)
+    exe = tmp_path / "thr"
+    subprocess.run([nvcc, "-std=c++17", "-O2", "-gencode", "arch=compute_100a,code=sm_100a",
+                    f"-I{CSRC}", str(src), "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert " 0 failed" in r.stdout

@@ -114,6 +114,9 @@ int fp64_shards(int64_t PL) {
 // Diagonals per lane: 8 amortises the per-column warp reduction best; fewer
 // only when the band count would leave SMs idle (>= 4 warps per SM wanted).
 int pick_fp64_R(int64_t ndiag) {
+#ifdef MPGPU_FP64_FORCE_R
+    return MPGPU_FP64_FORCE_R;  // tuning builds only
+#endif
     const int sms = sm_count();
     for (int R : {8, 4}) {
         const int64_t nb = (ndiag + 32 * R - 1) / (32 * R);
@@ -175,8 +178,18 @@ size_t fp64_scratch(int64_t n, int64_t m, int64_t ndiag, bool host_io) {
     b += align_up(8 * (size_t)std::max<int64_t>(ndiag, 1));  // first QT
     b += align_up(32 * (size_t)(PL + kFp64Pad)); // records
     b += 2 * align_up(8 * (size_t)PL * S);       // keys
+    b += align_up(8 * (size_t)(PL + kFp64ThrPad)); // selection thresholds
     if (host_io) b += align_up(8 * (size_t)PL) * 2;
     return b + 4096;
+}
+
+// Selection thresholds of the FP64 band join start at -DBL_MAX (every cell
+// selects until merges raise them).
+unsigned long long no_threshold_bits() {
+    const double v = -1.7976931348623157e308;
+    unsigned long long b;
+    std::memcpy(&b, &v, sizeof b);
+    return b;
 }
 
 // Guarded form, on top of fp32_scratch: hazard prefix counts and scan
@@ -341,6 +354,7 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
         double4* rec = cv.take<double4>(PL + kFp64Pad);
         unsigned long long* kex = cv.take<unsigned long long>(PL * shards);
         unsigned long long* kid = cv.take<unsigned long long>(PL * shards);
+        double* thr = cv.take<double>(PL + kFp64ThrPad);
         double* d2 = o_dev ? dist2_out : cv.take<double>(PL);
         int64_t* ix = o_dev ? idx_out : cv.take<int64_t>(PL);
 
@@ -348,7 +362,7 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
                                                            : cudaMemcpyHostToDevice, st));
         mark(ctx, 0, st);
         MP_CUDA(ctx, cudaMemsetAsync(Apad + n, 0, 8, st));
-        ref_prefix_kernel<<<1, 1, 0, st>>>(Apad, n, cs, cs2);
+        ref_prefix_kernel<<<1, kPrefixThreads, 0, st>>>(Apad, n, cs, cs2);
         MP_LAUNCHED(ctx);
         ref_stats_kernel<<<grid_for(PL), kThreads, 0, st>>>(cs, cs2, PL, m, muS, sInv);
         MP_LAUNCHED(ctx);
@@ -361,6 +375,9 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
         MP_LAUNCHED(ctx);
         MP_CUDA(ctx, cudaMemsetAsync(kex, 0, 8 * (size_t)PL * shards, st));
         MP_CUDA(ctx, cudaMemsetAsync(kid, 0, 8 * (size_t)PL * shards, st));
+        init_keys_kernel<<<grid_for(PL + kFp64ThrPad), kThreads, 0, st>>>(
+            reinterpret_cast<unsigned long long*>(thr), PL + kFp64ThrPad, no_threshold_bits());
+        MP_LAUNCHED(ctx);
         mark(ctx, 1, st);
         if (ndiag > 0) {
             Fp64BandParams P{};
@@ -383,6 +400,9 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
             P.floor = -1.0;
             P.idx_bits = bits_for((uint64_t)PL);
             P.key_vlo = key_vlo_bits(m);
+            P.thr = thr;
+            P.thr_eps = fp64_threshold_eps(P.idx_bits);
+            P.thr_tiny = fp64_threshold_tiny(P.m);
             launch_band(R, P, st);
             MP_LAUNCHED(ctx);
         }
@@ -567,7 +587,7 @@ int mp_window_stats(mp_context* ctx, const double* A, int64_t n, int64_t m, doub
     double* mu = cv.take<double>(PL);
     double* si = cv.take<double>(PL);
     MP_CUDA(ctx, cudaMemcpyAsync(Ad, A, 8 * n, cudaMemcpyDefault, st));
-    ref_prefix_kernel<<<1, 1, 0, st>>>(Ad, n, cs, cs2);
+    ref_prefix_kernel<<<1, kPrefixThreads, 0, st>>>(Ad, n, cs, cs2);
     MP_LAUNCHED(ctx);
     ref_stats_kernel<<<grid_for(PL), kThreads, 0, st>>>(cs, cs2, PL, m, mu, si);
     MP_LAUNCHED(ctx);
@@ -625,7 +645,7 @@ int mp_prescrimp(mp_context* ctx, const double* A, int64_t n, int64_t m, double 
     double* d2 = o_dev ? dist2_out : cv.take<double>(PL);
     int64_t* ix = o_dev ? idx_out : cv.take<int64_t>(PL);
     MP_CUDA(ctx, cudaMemcpyAsync(Ad, A, 8 * n, cudaMemcpyDefault, st));
-    ref_prefix_kernel<<<1, 1, 0, st>>>(Ad, n, cs, cs2);
+    ref_prefix_kernel<<<1, kPrefixThreads, 0, st>>>(Ad, n, cs, cs2);
     MP_LAUNCHED(ctx);
     orig_stats_kernel<<<grid_for(PL), kThreads, 0, st>>>(cs, cs2, PL, m, mean, sigma);
     MP_LAUNCHED(ctx);
@@ -735,7 +755,8 @@ int mp_eval_diag_block_triangle(mp_context* ctx, double* prof_colmin, int64_t* i
     const int64_t nq = std::min<int64_t>(blocklen, T);
     size_t need = 2 * align_up(32 * (size_t)nrec) + 2 * align_up(8 * (size_t)nq) +
                   2 * align_up(8 * (size_t)region) * 2 + 2 * align_up(8 * (size_t)(T + m)) +
-                  4 * align_up(8 * (size_t)T) + 4096;
+                  4 * align_up(8 * (size_t)T) + align_up(8 * (size_t)(region + kFp64ThrPad)) +
+                  4096;
     int rc = reserve(ctx, need);
     if (rc) return rc;
     Carve cv{(char*)ctx->arena};
@@ -753,6 +774,7 @@ int mp_eval_diag_block_triangle(mp_context* ctx, double* prof_colmin, int64_t* i
     double* mh = cv.take<double>(T);
     double* sv = cv.take<double>(T);
     double* mv = cv.take<double>(T);
+    double* thr = cv.take<double>(region + kFp64ThrPad);
     const cudaMemcpyKind K = cudaMemcpyDefault;
     MP_CUDA(ctx, cudaMemcpyAsync(ah, A_hor, 8 * (T + m), K, st));
     MP_CUDA(ctx, cudaMemcpyAsync(av, A_vert, 8 * (T + m), K, st));
@@ -777,6 +799,9 @@ int mp_eval_diag_block_triangle(mp_context* ctx, double* prof_colmin, int64_t* i
     pack_fp64_kernel<<<grid_for(T), kThreads, 0, st>>>(av, m, T, sv, mv, rowrec);
     MP_LAUNCHED(ctx);
     block_keys_init_kernel<<<grid_for(region), kThreads, 0, st>>>(prof, region, kex, kid);
+    MP_LAUNCHED(ctx);
+    init_keys_kernel<<<grid_for(region + kFp64ThrPad), kThreads, 0, st>>>(
+        reinterpret_cast<unsigned long long*>(thr), region + kFp64ThrPad, no_threshold_bits());
     MP_LAUNCHED(ctx);
 
     Fp64BandParams P{};
@@ -804,6 +829,9 @@ int mp_eval_diag_block_triangle(mp_context* ctx, double* prof_colmin, int64_t* i
     const int ib = bits_for((uint64_t)std::max(baserow + T, basecol + T));
     P.idx_bits = ib;
     P.key_vlo = key_vlo_bits(m);
+    P.thr = thr;
+    P.thr_eps = fp64_threshold_eps(ib);
+    P.thr_tiny = fp64_threshold_tiny(P.m);
     launch_band(R, P, st);
     MP_LAUNCHED(ctx);
     block_finalize_kernel<<<grid_for(region), kThreads, 0, st>>>(kex, kid, region, 1, region, ib,

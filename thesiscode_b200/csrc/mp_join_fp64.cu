@@ -21,11 +21,27 @@
 // accumulate in registers for R steps and then pass through a per-warp shared
 // memory ring (one writer per slot per chunk, no atomics) until the warp's
 // lowest lane has seen the row.  Finished rows and columns go to global
-// memory as 64-bit max reductions into one of several key shards.  Bands are
-// paired (k, nbands-1-k) per warp so every warp does the same work
-// (the reference's triv_par balance rule, ScrimpTrivialPar.cpp:200-224).
+// memory as 64-bit max reductions into one of several key shards.  One
+// resident wave of warps walks the bands in a snake order (band b to warp
+// b mod W in even rounds, W-1 - b mod W in odd ones), so every warp's bands
+// add up to nearly the same length -- the reference's triv_par balance rule
+// (ScrimpTrivialPar.cpp:200-224) carried over any number of rounds.
+//
+// Selection thresholds: every merge also raises a per-entry threshold to a
+// value just below the merged score (fp64_threshold_below: the margin is wider
+// than the index key's resolution).  A lane's row partials start at their
+// rows' thresholds, and in the branch-free chunks each column step first
+// evaluates its cells and compares them with their row partials and with the
+// column's threshold; only when some cell of the warp exceeds one does the
+// step run the (score, index) selection.  A cell that exceeds neither can
+// raise neither key of its row or column (its score is below a score already
+// merged there, by more than the index key resolves), so the result is the
+// same as selecting every cell.  Thresholds are read as they stand (a stale
+// one is only a lower bound), so the arithmetic and the keys -- and therefore
+// the output -- do not depend on timing.
 #include <float.h>
 
+#include <algorithm>
 #include <atomic>
 
 #include "mp_common.cuh"
@@ -52,25 +68,95 @@ __device__ __forceinline__ double4 ring_rec(const char* p) {
     return make_double4(u2d(a.x, a.y), u2d(a.z, a.w), u2d(b.x, b.y), u2d(b.z, b.w));
 }
 
+// A threshold as it stands (other warps raise it with atomics meanwhile; any
+// value it has held is a valid lower bound).
+__device__ __forceinline__ double ld_thr(const double* p) {
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+
 __device__ __forceinline__ void flush_fp64(const Fp64BandParams& P, int shard, int64_t slot,
                                            double score, int64_t neighbour) {
     unsigned long long* ke = P.kexact + (int64_t)shard * P.key_stride + slot;
     unsigned long long* ki = P.kidx + (int64_t)shard * P.key_stride + slot;
     atomicMax(ke, ord_f64(score));
     atomicMax(ki, idx_key_f64(score, P.m, (unsigned long long)neighbour, P.idx_bits, P.key_vlo));
+    // thresholds only ever hold non-negative values above their -DBL_MAX
+    // start, where the signed 64-bit pattern orders like the double
+    const double t = fp64_threshold_below(score, P.m, P.thr_eps, P.thr_tiny);
+    if (t >= 0.0) atomicMax(reinterpret_cast<long long*>(P.thr + slot), __double_as_longlong(t));
 }
 
-// One chunk = R consecutive columns.  Per column the lanes' best cells are
-// reduced across the warp with two REDUX instructions (high, then low word of
-// the ordered score); the lowest winning lane parks (score, row) in the
-// warp's column slot with a predicated store, so no divergent branch splits
-// consecutive steps.  The slots are flushed once per chunk.
+// Per-warp ring of row thresholds in shared memory, indexed like the record
+// ring (row t of the band at t % kRecRing), one double of padding after every
+// 8 so that lanes reading rows 8 apart hit distinct banks.
+constexpr int kThrRingDoubles = kRecRing + kRecRing / 8;
+__device__ __forceinline__ int thr_off(int t) {
+    const int s = t % kRecRing;
+    return s + (s >> 3);
+}
+
+// The (score, index) selection of one column step: row partials (strict '>',
+// the reference's rule; a partial started at its row's threshold keeps the
+// sentinel index -1 until a cell beats it), then the column's best cell over
+// the warp from two REDUX instructions (high, then low word of the ordered
+// score); the lowest winning lane parks (score, row) in the warp's column slot
+// with a predicated store, so no divergent branch splits consecutive steps.
+template <int R>
+__device__ __forceinline__ void select_step(const Fp64BandParams& P, int b, const double (&sc)[R],
+                                            double (&acc_s)[2 * R - 1], int (&acc_a)[2 * R - 1],
+                                            int64_t g0, int lane, double* cslot_s, int* cslot_r) {
+#pragma unroll
+    for (int a = 0; a < R; ++a) {
+        if (sc[a] > acc_s[b + a]) {
+            acc_s[b + a] = sc[a];
+            acc_a[b + a] = a;
+        }
+    }
+    // lane's best cell of the column: pairwise tree, left wins ties
+    double cb[R];
+    int ca[R];
+#pragma unroll
+    for (int a = 0; a < R; ++a) {
+        cb[a] = sc[a];
+        ca[a] = a;
+    }
+#pragma unroll
+    for (int w = 1; w < R; w *= 2)
+#pragma unroll
+        for (int a = 0; a + w < R; a += 2 * w)
+            if (cb[a + w] > cb[a]) {
+                cb[a] = cb[a + w];
+                ca[a] = ca[a + w];
+            }
+    const double cbest = cb[0];
+    const unsigned long long key = (cbest > P.floor) ? ord_f64(cbest) : 0ull;
+    const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+    const unsigned mhi = __reduce_max_sync(kFullMask, hi);
+    const unsigned mlo = __reduce_max_sync(kFullMask, hi == mhi ? lo : 0u);
+    const bool top = (hi == mhi) && (lo == mlo) && (mhi != 0u);
+    const unsigned tops = __ballot_sync(kFullMask, top);
+    if (top && (tops & ((1u << lane) - 1u)) == 0u) {
+        cslot_s[b] = cbest;
+        cslot_r[b] = (int)(b + g0 + ca[0]);  // row - jc (rows < 2^31)
+    }
+}
+
+// One chunk = R consecutive columns.  FAST chunks hold only cells of the
+// reference's 4-wide (fused) part; each step there evaluates its R cells per
+// lane, and the selection runs only when some cell of the warp exceeds its row
+// partial or the column's threshold cthr[b] (a warp vote).  Other chunks
+// evaluate every cell with its own geometry and always select.  Returns
+// whether any step selected (uniform over the warp).
 template <int R, bool FAST>
-__device__ __forceinline__ void chunk_fp64(const Fp64BandParams& P, int64_t jc, const char* rring,
+__device__ __forceinline__ bool chunk_fp64(const Fp64BandParams& P, int64_t jc, const char* rring,
                                            const char* rbase, int tbase, double4 (&rwin)[R], double (&qt)[R],
                                            const int (&len)[R], const int (&psw)[R],
                                            double (&acc_s)[2 * R - 1], int (&acc_a)[2 * R - 1],
-                                           int64_t g0, int lane, double* cslot_s, int* cslot_r) {
+                                           int64_t g0, int lane, double* cslot_s, int* cslot_r,
+                                           const double* cthr) {
+    bool selected = !FAST;
 #pragma unroll
     for (int b = 0; b < R; ++b) {
         const int64_t j = jc + b;
@@ -83,71 +169,56 @@ __device__ __forceinline__ void chunk_fp64(const Fp64BandParams& P, int64_t jc, 
                 ring_rec(rring + rec_off(rec_slot(tbase + b + R - 1)));
         const double4 cv = ld_rec(P.colrec + j);
         double sc[R];
+        if (FAST) {
+            const double tc = cthr[b];
+            bool hit = false;
 #pragma unroll
-        for (int a = 0; a < R; ++a) {
-            const double4 rv = rwin[(b + a) % R];
-            double score;
-            if (FAST) {
+            for (int a = 0; a < R; ++a) {
+                const double4 rv = rwin[(b + a) % R];
                 // 4-wide part of the reference kernel (kernels.cpp:206-225)
                 const double ss = __dmul_rn(rv.z, cv.z);
                 const double mm = __dmul_rn(cv.w, rv.w);
-                score = __fma_rn(qt[a], ss, -mm);
+                sc[a] = __fma_rn(qt[a], ss, -mm);
                 qt[a] = __fma_rn(-rv.x, cv.x, __fma_rn(rv.y, cv.y, qt[a]));
-            } else if (j < len[a]) {
-                const double ss = __dmul_rn(rv.z, cv.z);
-                if (j <= psw[a]) {
-                    const double mm = __dmul_rn(cv.w, rv.w);
-                    score = __fma_rn(qt[a], ss, -mm);
-                    qt[a] = __fma_rn(-rv.x, cv.x, __fma_rn(rv.y, cv.y, qt[a]));
+                hit |= (sc[a] > acc_s[b + a]) | (sc[a] > tc);
+            }
+            if (__any_sync(kFullMask, hit)) {
+                selected = true;
+                select_step<R>(P, b, sc, acc_s, acc_a, g0, lane, cslot_s, cslot_r);
+            }
+        } else {
+#pragma unroll
+            for (int a = 0; a < R; ++a) {
+                const double4 rv = rwin[(b + a) % R];
+                double score;
+                if (j < len[a]) {
+                    const double ss = __dmul_rn(rv.z, cv.z);
+                    if (j <= psw[a]) {
+                        const double mm = __dmul_rn(cv.w, rv.w);
+                        score = __fma_rn(qt[a], ss, -mm);
+                        qt[a] = __fma_rn(-rv.x, cv.x, __fma_rn(rv.y, cv.y, qt[a]));
+                    } else {
+                        // scalar remainder (kernels.cpp:282-289), no fusion
+                        score = __dsub_rn(__dmul_rn(qt[a], ss), __dmul_rn(rv.w, cv.w));
+                        qt[a] = __dsub_rn(__dadd_rn(qt[a], __dmul_rn(rv.y, cv.y)),
+                                          __dmul_rn(rv.x, cv.x));
+                    }
                 } else {
-                    // scalar remainder (kernels.cpp:282-289), no fusion
-                    score = __dsub_rn(__dmul_rn(qt[a], ss), __dmul_rn(rv.w, cv.w));
-                    qt[a] = __dsub_rn(__dadd_rn(qt[a], __dmul_rn(rv.y, cv.y)),
-                                      __dmul_rn(rv.x, cv.x));
+                    score = -DBL_MAX;
                 }
-            } else {
-                score = -DBL_MAX;
+                sc[a] = score;
             }
-            sc[a] = score;
-            if (score > acc_s[b + a]) {
-                acc_s[b + a] = score;
-                acc_a[b + a] = a;
-            }
-        }
-        // lane's best cell of column j: pairwise tree, left wins ties
-        double cb[R];
-        int ca[R];
-#pragma unroll
-        for (int a = 0; a < R; ++a) {
-            cb[a] = sc[a];
-            ca[a] = a;
-        }
-#pragma unroll
-        for (int w = 1; w < R; w *= 2)
-#pragma unroll
-            for (int a = 0; a + w < R; a += 2 * w)
-                if (cb[a + w] > cb[a]) {
-                    cb[a] = cb[a + w];
-                    ca[a] = ca[a + w];
-                }
-        const double cbest = cb[0];
-        const unsigned long long key = (cbest > P.floor) ? ord_f64(cbest) : 0ull;
-        const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
-        const unsigned mhi = __reduce_max_sync(kFullMask, hi);
-        const unsigned mlo = __reduce_max_sync(kFullMask, hi == mhi ? lo : 0u);
-        const bool top = (hi == mhi) && (lo == mlo) && (mhi != 0u);
-        const unsigned tops = __ballot_sync(kFullMask, top);
-        if (top && (tops & ((1u << lane) - 1u)) == 0u) {
-            cslot_s[b] = cbest;
-            cslot_r[b] = (int)(j + g0 + ca[0] - jc);  // row - jc, small and non-negative
+            select_step<R>(P, b, sc, acc_s, acc_a, g0, lane, cslot_s, cslot_r);
         }
     }
+    return selected;
 }
 
 template <int R>
 __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band, int lane,
                                           int shard, double* ring_s, int* ring_c, char* rring,
-                                          double* cslot_s, int* cslot_r) {
+                                          double* cslot_s, int* cslot_r, double* tring,
+                                          double* cthr) {
     constexpr int RING = 32 * R;
     const int64_t gb = P.g_lo + band * (int64_t)RING;
     const int64_t g0 = gb + (int64_t)lane * R;
@@ -180,42 +251,53 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
         ring_c[k] = 0;
     }
     if (lane < R) cslot_s[lane] = -DBL_MAX;
-    __syncwarp();
 
-    double acc_s[2 * R - 1];
-    int acc_a[2 * R - 1];
-#pragma unroll
-    for (int k = 0; k < 2 * R - 1; ++k) {
-        acc_s[k] = -DBL_MAX;
-        acc_a[k] = 0;
-    }
-
-    // row records of the band (t = row - gb) staged in the warp's shared-memory
-    // ring; before chunk jc it holds t < fill
+    // row records of the band (t = row - gb) and their rows' thresholds staged
+    // in the warp's shared-memory rings; before chunk jc they hold t < fill
     const uint4* rsrc = reinterpret_cast<const uint4*>(P.rowrec + gb);
+    const double* tsrc = P.thr + gb + P.row_key_off;  // threshold of band row t
+    const double* csrc = P.thr + P.col_key_off;       // threshold of column j
     int fill = 34 * R;
     for (int i = lane; i < 2 * fill; i += 32) rec_store(rring, i >> 1, i & 1, __ldg(rsrc + i));
+    for (int i = lane; i < fill; i += 32) tring[thr_off(i)] = ld_thr(tsrc + i);
+    if (lane < R) cthr[lane] = ld_thr(csrc + lane);
     __syncwarp();
     // register window of row records: slot (k mod R) holds row g0 + jc + k
     double4 rwin[R];
 #pragma unroll
     for (int k = 0; k < R - 1; ++k) rwin[k] = ring_rec(rring + rec_off(rec_slot(lane * R + k)));
+    // row partials: slot k holds row g0 + jc + k, starting at the row's
+    // threshold with the sentinel index -1 (no candidate yet)
+    double acc_s[2 * R - 1];
+    int acc_a[2 * R - 1];
+#pragma unroll
+    for (int k = 0; k < 2 * R - 1; ++k) {
+        acc_s[k] = tring[thr_off(lane * R + k)];
+        acc_a[k] = -1;
+    }
 
+    bool sel_prev = false;
     for (int64_t jc = 0; jc < jmax; jc += R) {
         uint4 next = make_uint4(0, 0, 0, 0);
         if (lane < 2 * R) next = __ldg(rsrc + 2 * fill + lane);
+        double tnext = 0.0, cnext = 0.0;  // next rows' and next chunk's column thresholds
+        if (lane < R) {
+            tnext = ld_thr(tsrc + fill + lane);
+            cnext = ld_thr(csrc + jc + R + lane);
+        }
         const int tbase = (int)jc + lane * R;
         const char* rbase = rring + rec_off(rec_slot(tbase + R - 1));
         const bool fast = __all_sync(kFullMask, jc + R - 1 <= minpsw);
+        bool sel;
         if (fast)
-            chunk_fp64<R, true>(P, jc, rring, rbase, tbase, rwin, qt, len, psw, acc_s, acc_a, g0, lane,
-                                cslot_s, cslot_r);
+            sel = chunk_fp64<R, true>(P, jc, rring, rbase, tbase, rwin, qt, len, psw, acc_s, acc_a,
+                                      g0, lane, cslot_s, cslot_r, cthr);
         else
-            chunk_fp64<R, false>(P, jc, rring, rbase, tbase, rwin, qt, len, psw, acc_s, acc_a, g0, lane,
-                                 cslot_s, cslot_r);
+            sel = chunk_fp64<R, false>(P, jc, rring, rbase, tbase, rwin, qt, len, psw, acc_s, acc_a,
+                                       g0, lane, cslot_s, cslot_r, cthr);
         __syncwarp();
         // the chunk's column maxima (one per column, parked by the winning lane)
-        if (lane < R) {
+        if (sel && lane < R) {
             const double cs = cslot_s[lane];
             if (cs > P.floor)
                 flush_fp64(P, shard, jc + lane + P.col_key_off, cs,
@@ -223,16 +305,24 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
             cslot_s[lane] = -DBL_MAX;
         }
         if (lane < 2 * R) rec_store(rring, fill + (lane >> 1), lane & 1, next);
+        if (lane < R) {
+            tring[thr_off(fill + lane)] = tnext;
+            cthr[lane] = cnext;
+        }
         fill += R;
-        // rows jc + g0 + [0, R) are done for this lane: merge into the ring
-        const int base = (int)(((jc / R) + lane) % 32) * R;
+        // rows jc + g0 + [0, R) are done for this lane: merge its candidates
+        // (selected in this chunk or the previous one) into the ring
+        if (sel || sel_prev) {
+            const int base = (int)(((jc / R) + lane) % 32) * R;
 #pragma unroll
-        for (int k = 0; k < R; ++k) {
-            if (acc_s[k] > ring_s[base + k]) {
-                ring_s[base + k] = acc_s[k];
-                ring_c[base + k] = (int)(jc + k - acc_a[k]);
+            for (int k = 0; k < R; ++k) {
+                if (acc_a[k] >= 0 && acc_s[k] > ring_s[base + k]) {
+                    ring_s[base + k] = acc_s[k];
+                    ring_c[base + k] = (int)(jc + k - acc_a[k]);
+                }
             }
         }
+        sel_prev = sel;
         __syncwarp();
         // rows jc + gb + [0, R) have now met every lane: flush and free
         if (lane < R) {
@@ -248,8 +338,12 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
             acc_s[k] = acc_s[k + R];
             acc_a[k] = acc_a[k + R];
         }
+        // new rows jc + R + g0 + k start at their thresholds
 #pragma unroll
-        for (int k = R - 1; k < 2 * R - 1; ++k) acc_s[k] = -DBL_MAX;
+        for (int k = R - 1; k < 2 * R - 1; ++k) {
+            acc_s[k] = tring[thr_off(tbase + R + k)];
+            acc_a[k] = -1;
+        }
     }
 
     // drain: carried rows jend + g0 + [0, R-1) into the ring, then every slot
@@ -257,7 +351,7 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
     const int base = (int)(((jend / R) + lane) % 32) * R;
 #pragma unroll
     for (int k = 0; k < R - 1; ++k) {
-        if (acc_s[k] > ring_s[base + k]) {
+        if (acc_a[k] >= 0 && acc_s[k] > ring_s[base + k]) {
             ring_s[base + k] = acc_s[k];
             ring_c[base + k] = (int)(jend + k - acc_a[k]);
         }
@@ -282,7 +376,8 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
 template <int R>
 constexpr int fp64_smem_bytes() {
     return kFp64WarpsPerBlock *
-           (kRecRingBytes + (32 * R + R) * (int)(sizeof(double) + sizeof(int)));
+           (kRecRingBytes + (32 * R + R) * (int)(sizeof(double) + sizeof(int)) +
+            (kThrRingDoubles + R) * (int)sizeof(double));
 }
 
 template <int R>
@@ -290,42 +385,62 @@ __global__ void __launch_bounds__(32 * kFp64WarpsPerBlock) fp64_band_kernel(cons
     extern __shared__ __align__(128) char smem_fp64[];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
-    char* rring = smem_fp64 + w * kRecRingBytes;
-    double* ring_s = reinterpret_cast<double*>(smem_fp64 + kFp64WarpsPerBlock * kRecRingBytes) +
-                     w * 32 * R;
-    int* ring_c = reinterpret_cast<int*>(smem_fp64 + kFp64WarpsPerBlock * kRecRingBytes +
-                                         kFp64WarpsPerBlock * 32 * R * sizeof(double)) +
-                  w * 32 * R;
-    double* cslot_s = reinterpret_cast<double*>(
-                          smem_fp64 + kFp64WarpsPerBlock * kRecRingBytes +
-                          kFp64WarpsPerBlock * 32 * R * (sizeof(double) + sizeof(int))) +
-                      w * R;
-    int* cslot_r = reinterpret_cast<int*>(cslot_s + (kFp64WarpsPerBlock - w) * R) + w * R;
-    const int64_t job = (int64_t)blockIdx.x * kFp64WarpsPerBlock + w;
-    const int64_t njobs = (P.nbands + 1) / 2;
-    if (job >= njobs) return;
-    const int shard = (int)(job % P.shards);
-    band_fp64<R>(P, job, lane, shard, ring_s, ring_c, rring, cslot_s, cslot_r);
-    const int64_t partner = P.nbands - 1 - job;
-    if (partner > job) band_fp64<R>(P, partner, lane, shard, ring_s, ring_c, rring, cslot_s, cslot_r);
+    constexpr int kW = kFp64WarpsPerBlock;
+    char* p = smem_fp64;
+    char* rring = p + w * kRecRingBytes;
+    p += kW * kRecRingBytes;
+    double* tring = reinterpret_cast<double*>(p) + w * kThrRingDoubles;
+    p += kW * kThrRingDoubles * sizeof(double);
+    double* ring_s = reinterpret_cast<double*>(p) + w * 32 * R;
+    p += kW * 32 * R * sizeof(double);
+    double* cslot_s = reinterpret_cast<double*>(p) + w * R;
+    p += kW * R * sizeof(double);
+    double* cthr = reinterpret_cast<double*>(p) + w * R;
+    p += kW * R * sizeof(double);
+    int* ring_c = reinterpret_cast<int*>(p) + w * 32 * R;
+    p += kW * 32 * R * sizeof(int);
+    int* cslot_r = reinterpret_cast<int*>(p) + w * R;
+    // One resident wave of W warps.  Band b (longest first: band lengths fall
+    // with b) goes to warp b mod W in even rounds and W-1 - (b mod W) in odd
+    // rounds, so every warp's bands add up to nearly the same length -- the
+    // reference's (k, nbands-1-k) pairing carried over any number of rounds.
+    const int64_t W = (int64_t)gridDim.x * kFp64WarpsPerBlock;
+    const int64_t wid = (int64_t)blockIdx.x * kFp64WarpsPerBlock + w;
+    const int shard = (int)(wid % P.shards);
+    for (int64_t r = 0;; ++r) {
+        const int64_t band = r * W + ((r & 1) ? W - 1 - wid : wid);
+        if (band >= P.nbands) break;
+        band_fp64<R>(P, band, lane, shard, ring_s, ring_c, rring, cslot_s, cslot_r, tring, cthr);
+    }
 }
 
 }  // namespace
 
 template <int R>
 void launch_fp64_band(const Fp64BandParams& P, cudaStream_t s) {
-    const int64_t njobs = (P.nbands + 1) / 2;
-    const int64_t blocks = (njobs + kFp64WarpsPerBlock - 1) / kFp64WarpsPerBlock;
     constexpr int smem = fp64_smem_bytes<R>();
-    // per-device attribute, idempotent: see launch_fp32_join
+    // per-device attribute and occupancy, idempotent: see launch_fp32_join
     static std::atomic<unsigned long long> configured{0};
+    static std::atomic<int> resident[64];
     int dev = 0;
     cudaGetDevice(&dev);
     const unsigned long long bit = 1ull << (dev & 63);
     if (!(configured.load(std::memory_order_acquire) & bit)) {
         cudaFuncSetAttribute(fp64_band_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fp64_band_kernel<R>,
+                                                          32 * kFp64WarpsPerBlock, smem) != cudaSuccess ||
+            per_sm < 1) {
+            cudaGetLastError();
+            per_sm = 1;
+        }
+        resident[dev & 63].store(per_sm, std::memory_order_relaxed);
         configured.fetch_or(bit, std::memory_order_release);
     }
+    // one resident wave, fewer CTAs when there are fewer bands than warps
+    const int64_t wave = (int64_t)sm_count() * resident[dev & 63].load(std::memory_order_relaxed);
+    const int64_t want = (P.nbands + kFp64WarpsPerBlock - 1) / kFp64WarpsPerBlock;
+    const int64_t blocks = std::min<int64_t>(want, wave);
     if (blocks > 0) fp64_band_kernel<R><<<(unsigned)blocks, 32 * kFp64WarpsPerBlock, smem, s>>>(P);
 }
 

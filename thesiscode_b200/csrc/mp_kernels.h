@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cmath>
+
 struct mp_context;
 
 namespace mpgpu {
@@ -14,6 +16,8 @@ size_t ctx_budget(const mp_context* ctx);
 int ctx_device(const mp_context* ctx);
 
 // ---- preparation (mp_prep.cu) ----------------------------------------------
+constexpr int kPrefixThreads = 256;  // ref_prefix_kernel: one block of this many threads
+constexpr int kPrefixChunk = 1024;   // elements of A per shared-memory chunk
 __global__ void ref_prefix_kernel(const double* A, int64_t n, double* cs, double* cs2);
 __global__ void ref_stats_kernel(const double* cs, const double* cs2, int64_t PL, int64_t m,
                                  double* muS, double* sInv);
@@ -53,8 +57,31 @@ struct Fp64BandParams {
     double floor;  // only scores strictly above it are merged (-1: reference init)
     int idx_bits;
     long long key_vlo;  // bit pattern of the index key's lower range end (idx_key_f64)
+    // Selection thresholds, one per key slot plus kFp64ThrPad slots of padding
+    // (initialised to -DBL_MAX).  Every merge raises thr[slot] to a value a
+    // little below the merged score (fp64_threshold_below); a cell whose score
+    // does not exceed its row's and its column's thresholds can change neither
+    // key, so a column step whose cells all fall below them skips selection.
+    double* thr;
+    double thr_eps;   // relative margin, wider than the index key's resolution
+    double thr_tiny;  // absolute margin near v = m - score = 0
 };
 constexpr int kFp64WarpsPerBlock = 4;
+constexpr int64_t kFp64ThrPad = 64 * 8 + 64;  // >= the 34R + R rows staged past a band's end
+// Threshold stored after merging `score` (see Fp64BandParams::thr): below the
+// score by more than the index key's resolution, so every cell whose index key
+// could still tie or beat the key of a merged cell exceeds it.  Host-callable
+// so the margin can be checked without a GPU.
+__host__ __device__ inline double fp64_threshold_below(double score, double m, double eps,
+                                                       double tiny) {
+    const double v = m - score > 0.0 ? m - score : 0.0;
+    return m - (v * (1.0 + eps) + tiny);
+}
+// Margins for a key with idx_bits index bits: the index key keeps 57 - idx_bits
+// mantissa bits of v, i.e. a relative resolution of 2^(idx_bits - 57); eps is
+// eight times that, tiny covers |v| near 0, where the key clamps.
+inline double fp64_threshold_eps(int idx_bits) { return std::ldexp(1.0, idx_bits - 54); }
+inline double fp64_threshold_tiny(double m) { return std::ldexp(m, -40); }
 template <int R>
 void launch_fp64_band(const Fp64BandParams& P, cudaStream_t s);
 

@@ -20,33 +20,68 @@ namespace mpgpu {
 // ---- reference-exact statistics -------------------------------------------
 
 // cs[i] = A[i] + cs[i-1], cs2[i] = A[i]*A[i] + cs2[i-1] in index order
-// (ScrimpSequOpt.cpp:43-49).  One thread: the chain is inherently serial.
-__global__ void ref_prefix_kernel(const double* __restrict__ A, int64_t n, double* __restrict__ cs,
-                                  double* __restrict__ cs2) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    double s = A[0];
-    double s2 = __dmul_rn(A[0], A[0]);
-    cs[0] = s;
-    cs2[0] = s2;
-    int64_t i = 1;
-    for (; i + 8 <= n; i += 8) {
-        double a[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) a[k] = __ldg(A + i + k);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            s = __dadd_rn(a[k], s);
-            s2 = __dadd_rn(__dmul_rn(a[k], a[k]), s2);
-            cs[i + k] = s;
-            cs2[i + k] = s2;
+// (ScrimpSequOpt.cpp:43-49).  The chain is inherently serial, so one thread
+// runs it -- out of shared memory: the block's other warps load the next chunk
+// of A and write the previous chunk's sums back (both coalesced) while thread 0
+// walks the current one, so the chain never waits for global memory.  Launch
+// with kPrefixThreads threads in one block.
+__global__ void __launch_bounds__(kPrefixThreads)
+    ref_prefix_kernel(const double* __restrict__ A, int64_t n, double* __restrict__ cs,
+                      double* __restrict__ cs2) {
+    constexpr int C = kPrefixChunk;
+    __shared__ double in[2][C];
+    __shared__ double o1[2][C];
+    __shared__ double o2[2][C];
+    if (blockIdx.x != 0) return;
+    const int t = threadIdx.x;
+    const int64_t nch = (n + C - 1) / C;
+    for (int k = t; k < C; k += blockDim.x) in[0][k] = k < n ? A[k] : 0.0;
+    __syncthreads();
+    double s = 0.0, s2 = 0.0;
+    for (int64_t c = 0; c < nch; ++c) {
+        const int b = (int)(c & 1);
+        if (t == 0) {
+            const int64_t base = c * C;
+            const int cnt = (int)min((int64_t)C, n - base);
+            int k = 0;
+            if (base == 0) {
+                s = in[b][0];
+                s2 = __dmul_rn(s, s);
+                o1[b][0] = s;
+                o2[b][0] = s2;
+                k = 1;
+            }
+#pragma unroll 8
+            for (; k < cnt; ++k) {
+                const double a = in[b][k];
+                s = __dadd_rn(a, s);
+                s2 = __dadd_rn(__dmul_rn(a, a), s2);
+                o1[b][k] = s;
+                o2[b][k] = s2;
+            }
+        } else if (t >= 32) {
+            const int tt = t - 32, nt = blockDim.x - 32;
+            if (c + 1 < nch)
+                for (int k = tt; k < C; k += nt) {
+                    const int64_t i = (c + 1) * C + k;
+                    in[b ^ 1][k] = i < n ? A[i] : 0.0;
+                }
+            if (c >= 1)
+                for (int k = tt; k < C; k += nt) {
+                    const int64_t i = (c - 1) * C + k;
+                    cs[i] = o1[b ^ 1][k];
+                    cs2[i] = o2[b ^ 1][k];
+                }
         }
+        __syncthreads();
     }
-    for (; i < n; ++i) {
-        const double a = A[i];
-        s = __dadd_rn(a, s);
-        s2 = __dadd_rn(__dmul_rn(a, a), s2);
-        cs[i] = s;
-        cs2[i] = s2;
+    const int64_t c = nch - 1;
+    for (int k = t; k < C; k += blockDim.x) {
+        const int64_t i = c * C + k;
+        if (i < n) {
+            cs[i] = o1[c & 1][k];
+            cs2[i] = o2[c & 1][k];
+        }
     }
 }
 
