@@ -552,7 +552,8 @@ def main():
     ap.add_argument("--c4-count", type=int, default=4096)
     ap.add_argument("--rates", type=float, nargs="+", default=[10, 30, 100, 300])
     ap.add_argument("--serve-seconds", type=float, default=10.0)
-    ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--slots", type=int, default=32,
+                    help="requests the server keeps admitted at once (c5)")
     ap.add_argument("--reanchor-k", type=int, default=1024)
     ap.add_argument("--fp64-steps", type=int, default=3)
     ap.add_argument("--ref-seconds", type=float, default=8.0)

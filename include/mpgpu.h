@@ -169,12 +169,23 @@ int mp_batch_run(mp_batch* b, const void* const* series, double* const* dist2_ou
 
 /*
  * Request server (no counterpart in the reference).  Continuous batching of
- * independent self-joins: requests are admitted in arrival order as soon as one
- * of `slots` workers is free and the device memory they need (scratch +
- * resident result, see mp_selfjoin_scratch_bytes) fits in mem_budget_bytes;
- * admitted requests run concurrently on their own streams.  A finished profile
- * stays on the device until mp_server_collect copies it out (and frees it).
- * A request larger than the whole budget is rejected (MP_ERR_BUDGET).
+ * independent self-joins: requests are admitted in arrival order while fewer
+ * than `slots` are admitted and the device memory they need (scratch +
+ * resident result) fits in mem_budget_bytes.  A finished profile stays on the
+ * device until mp_server_collect copies it out (and frees it).  A request
+ * larger than the whole budget is rejected (MP_ERR_BUDGET).
+ *   MP_PREC_FP32_REANCHOR  one scheduler runs every admitted request as part
+ *                          of epochs: one persistent launch of the FP32 tile
+ *                          kernel over a bounded slice of tiles from each
+ *                          (a minimum share each, the rest to the requests
+ *                          with the least work left); new requests join the
+ *                          next epoch.  Device memory comes from a pool of
+ *                          the server's own (stream-ordered, kept between
+ *                          requests, bounded by the budget).  Results equal
+ *                          mp_selfjoin's with the same reanchor_k.
+ *   MP_PREC_FP64, MP_PREC_FP32_GUARDED
+ *                          `slots` worker threads run whole mp_selfjoin calls,
+ *                          each on its own stream.
  *   mp_server_submit   copies the host series, returns a ticket, never blocks
  *   mp_server_poll     1 when finished (status set), 0 while pending
  *   mp_server_collect  waits for the ticket, copies d2/idx (may be NULL), frees;

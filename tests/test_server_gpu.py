@@ -1,7 +1,11 @@
 """Continuous-batching server: results are identical alone and in the mix
-(requests admitted while others run, overlapping on the device), admission
-respects the memory budget, oversized requests are rejected."""
+(requests admitted while others run, overlapping on the device) and equal to
+mp_selfjoin's, a small request that arrives while a large one runs finishes
+first, admission respects the memory budget, oversized requests are
+rejected."""
 from __future__ import annotations
+
+import time
 
 import numpy as np
 import pytest
@@ -46,13 +50,44 @@ def test_same_result_alone_and_in_the_mix(oracle):
     for kind, t in tickets:
         if kind == "o":
             assert srv.collect(t, want_profile=False)[0] == mp.MP_OK
+    ctx = mp.Context(0)
     for a, b, (x, m) in zip(alone, mixed, reqs):
         assert np.array_equal(a.dist2, b.dist2) and np.array_equal(a.index, b.index)
+        want = ctx.selfjoin(x, m, precision=mp.FP32_REANCHOR, reanchor_k=1024)
+        assert np.array_equal(a.dist2, want.dist2) and np.array_equal(a.index, want.index)
         d2, _ = oracle.selfjoin(x, m)
         rel = np.abs(np.sqrt(np.abs(b.dist2)) - np.sqrt(d2)) / np.sqrt(d2)
         assert rel.max() <= 1e-4
+    ctx.close()
     st = srv.stats()
     assert st["completed"] == len(reqs) * 2 + len(others) and st["bytes_in_use"] == 0
+    srv.close()
+
+
+def test_small_request_overtakes_a_large_one():
+    """Requests share the device epoch by epoch: a small request submitted while
+    a large one is running finishes long before it, with the same profile as
+    when it runs alone."""
+    big, m_big = workloads.random_walk(1_048_576, 11), 128
+    small, m_small = workloads.random_walk(20_000, 12), 64
+    srv = mp.Server(0, 8 << 30, slots=4)
+    t_alone, _ = srv.submit(small, m_small)
+    alone = srv.collect(t_alone)[1]
+    t0 = time.perf_counter()
+    tb, rc = srv.submit(big, m_big)
+    assert rc == mp.MP_OK
+    time.sleep(0.03)  # the large join is on the device now
+    assert not srv.done(tb)
+    ts, rc = srv.submit(small, m_small)
+    dt = time.perf_counter() - t0
+    assert rc == mp.MP_OK
+    rs = srv.collect(ts)
+    assert not srv.done(tb), "the large request finished before the small one"
+    rb = srv.collect(tb, want_profile=False)
+    assert rs[0] == mp.MP_OK and rb[0] == mp.MP_OK
+    # finish times, both measured from the large request's submission
+    assert dt + rs[2] < 0.5 * rb[2], (dt, rs[2], rb[2])
+    assert np.array_equal(rs[1].dist2, alone.dist2) and np.array_equal(rs[1].index, alone.index)
     srv.close()
 
 

@@ -390,8 +390,10 @@ class Batch:
 
 class Server:
     """Continuous-batching request server (mp_server_*): submit self-joins,
-    collect profiles; admission by device-memory budget, `slots` concurrent
-    workers each on its own stream."""
+    collect profiles; admission by device-memory budget, at most `slots`
+    requests admitted at once.  The FP32 re-anchored form runs the admitted
+    requests together as epochs of the persistent tile kernel; the FP64 and
+    guarded forms run `slots` workers, each on its own stream."""
 
     def __init__(self, device: int = 0, mem_budget_bytes: int = 8 << 30, slots: int = 4,
                  precision: int = FP32_REANCHOR, reanchor_k: int = 1024):

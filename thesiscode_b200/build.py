@@ -23,7 +23,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SOURCES = ["mp_prep.cu", "mp_join_fp64.cu", "mp_join_fp32.cu", "mp_finalize.cu",
                 "mp_capi.cu", "mp_calib.cu", "mp_batch.cu", "mp_noalloc.cu", "mp_prescrimp.cu",
-                "mp_guard.cu"]
+                "mp_guard.cu", "mp_serve.cu"]
 HOST_SOURCES = ["host/matprof_algo.cpp", "host/gpu_variants.cpp", "host/profile_io.cpp",
                 "host/mp_server.cpp"]
 CLI_SOURCES = ["host/main.cpp"]

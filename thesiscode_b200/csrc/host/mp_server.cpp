@@ -1,13 +1,24 @@
 // Self-join request server: continuous batching of independent self-joins.
 //
-// Requests are admitted in arrival order as soon as a worker slot is free and
-// the device memory they need (scratch + their resident result) fits in the
-// server's budget; admitted requests run concurrently, each worker on its own
-// CUDA stream and context, so the GPU overlaps their kernels.  A finished
-// profile stays in device memory until the client collects it, and its memory
-// counts against the budget until then.  A request larger than the whole
-// budget is rejected at submission.  No counterpart in the reference (one
-// join per process there).
+// Requests are admitted in arrival order as soon as the server has a free
+// slot and the device memory they need (scratch + their resident result) fits
+// in its budget.  A finished profile stays in device memory until the client
+// collects it, and its memory counts against the budget until then.  A request
+// larger than the whole budget is rejected at submission.  No counterpart in
+// the reference (one join per process there).
+//
+// FP32 re-anchored form: one scheduler thread runs the admitted requests as
+// epochs (mp_serve.h).  Each epoch is one persistent launch of the FP32 tile
+// kernel over a bounded slice of tiles (about kEpochCells cells) drawn from
+// every admitted request: each request first gets a minimum share, then the
+// rest goes to the requests with the least work left, so a small request
+// that arrives while a large one runs is finished within an epoch or two.
+// New requests are prepared on the same stream between epochs; two epochs are
+// kept in flight so the GPU never waits for the scheduler.  Device memory
+// comes from a server-owned stream-ordered pool, so no allocation or release
+// waits for the device.
+// FP64 and guarded FP32 forms: worker threads, each running whole
+// mp_selfjoin calls on its own stream and context.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -21,6 +32,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "mp_serve.h"
 #include "mpgpu.h"
 
 namespace {
@@ -38,6 +50,7 @@ struct Request {
     double* d_d2 = nullptr;
     int64_t* d_idx = nullptr;
     bool collected = false;
+    mpgpu::ServeJob job;  // epoch mode
 };
 
 }  // namespace
@@ -58,6 +71,12 @@ struct mp_server {
     int64_t next_id = 1;
     bool stop = false;
     std::vector<std::thread> workers;
+    // epoch mode (FP32 re-anchored form)
+    bool epochs = false;
+    int slots = 0;
+    std::thread engine;
+    cudaMemPool_t pool = nullptr;
+    int64_t epochs_launched = 0;
     // statistics
     int64_t completed = 0, rejected = 0;
     double cells_done = 0.0;
@@ -143,6 +162,197 @@ void worker_main(mp_server* s) {
     cudaStreamDestroy(st);
 }
 
+// ---- epoch mode -------------------------------------------------------------
+
+// Cells per epoch: about 4 ms of the FP32 tile kernel on a B200 -- short enough
+// that a new request waits little, long enough that the launch tail (warps
+// running out of tiles) stays a few percent.
+constexpr double kEpochCells = 1.2e10;
+constexpr int kEpochsInFlight = 2;
+
+// Picks the epoch's slices: every request with tiles left first gets a
+// minimum share (a quarter of the epoch split evenly), then the remaining
+// budget goes to the requests with the fewest cells left.
+std::vector<mpgpu::ServeSlice> choose_slices(std::vector<Request*>& act) {
+    std::vector<mpgpu::ServeSlice> out;
+    std::vector<Request*> open;
+    for (Request* r : act)
+        if (r->job.next_tile < r->job.ntiles) open.push_back(r);
+    if (open.empty()) return out;
+    auto tile_cells = [](const mpgpu::ServeJob& j) { return 256.0 * (double)j.K; };
+    auto left_cells = [&](const Request* r) {
+        return (double)(r->job.ntiles - r->job.next_tile) * tile_cells(r->job);
+    };
+    std::stable_sort(open.begin(), open.end(),
+                     [&](const Request* a, const Request* b) { return left_cells(a) < left_cells(b); });
+    std::vector<int64_t> give(open.size(), 0);
+    double budget = kEpochCells;
+    const double share = kEpochCells / (4.0 * (double)open.size());
+    for (size_t i = 0; i < open.size(); ++i) {
+        const mpgpu::ServeJob& j = open[i]->job;
+        const int64_t left = j.ntiles - j.next_tile;
+        const int64_t t = std::min<int64_t>(left, std::max<int64_t>(1, (int64_t)(share / tile_cells(j))));
+        give[i] = t;
+        budget -= (double)t * tile_cells(j);
+    }
+    for (size_t i = 0; i < open.size() && budget > 0; ++i) {
+        const mpgpu::ServeJob& j = open[i]->job;
+        const int64_t left = j.ntiles - j.next_tile - give[i];
+        const int64_t t = std::min<int64_t>(left, (int64_t)(budget / tile_cells(j)));
+        if (t <= 0) continue;
+        give[i] += t;
+        budget -= (double)t * tile_cells(j);
+    }
+    for (size_t i = 0; i < open.size(); ++i)
+        if (give[i] > 0) out.push_back({&open[i]->job, open[i]->job.next_tile, give[i]});
+    return out;
+}
+
+// Marks requests finished (their last epoch and finalisation are done).
+void complete_locked(mp_server* s, const std::vector<Request*>& done, int status) {
+    const Clock::time_point now = Clock::now();
+    for (Request* r : done) {
+        r->finished = now;
+        r->status = status;
+        const size_t keep = (status == MP_OK) ? mpgpu::serve_result_bytes(r->job.n, r->m) : 0;
+        s->in_use -= r->accounted - keep;
+        r->accounted = keep;
+        ++s->free_slots;
+        if (status == MP_OK) {
+            ++s->completed;
+            s->cells_done += r->job.cells;
+        }
+    }
+    admit_locked(s);
+}
+
+void engine_main(mp_server* s) {
+    cudaSetDevice(s->device);
+    cudaStream_t st;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    mpgpu::ServeEpochBuffers eb;
+    const cudaError_t be = mpgpu::serve_epoch_buffers_create(eb, s->slots);
+    struct InFlight {
+        cudaEvent_t ev;
+        std::vector<Request*> finishing;
+    };
+    std::deque<InFlight> inflight;
+    std::vector<Request*> active;  // prepared, tiles left to launch
+    std::vector<cudaEvent_t> spare;
+    auto retire_front = [&]() {
+        InFlight f = std::move(inflight.front());
+        inflight.pop_front();
+        const int status = cudaEventSynchronize(f.ev) == cudaSuccess ? MP_OK : MP_ERR_CUDA;
+        spare.push_back(f.ev);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            for (Request* r : f.finishing) {
+                r->series.clear();
+                r->series.shrink_to_fit();
+            }
+            complete_locked(s, f.finishing, status);
+        }
+        s->cv_done.notify_all();
+    };
+    for (;;) {
+        std::vector<Request*> fresh;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            const bool busy = !inflight.empty() ||
+                              std::any_of(active.begin(), active.end(), [](const Request* r) {
+                                  return r->job.next_tile < r->job.ntiles;
+                              });
+            if (!busy)
+                s->cv_work.wait(lk, [&] { return s->stop || !s->admitted.empty(); });
+            if (s->stop && s->admitted.empty() && !busy) break;
+            while (!s->admitted.empty()) {
+                Request* r = s->reqs[s->admitted.front()].get();
+                s->admitted.pop_front();
+                r->started = Clock::now();
+                fresh.push_back(r);
+            }
+        }
+        // new requests: device buffers from the pool, series in, preparation
+        std::vector<Request*> failed, finishing;
+        for (Request* r : fresh) {
+            cudaError_t e = be;
+            if (e == cudaSuccess)
+                e = mpgpu::serve_prepare(r->job, r->series.data(), (int64_t)r->series.size(), r->m,
+                                         s->reanchor_k, s->pool, st);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                mpgpu::serve_release_result(r->job, st);
+                failed.push_back(r);
+                continue;
+            }
+            r->d_d2 = r->job.d2;
+            r->d_idx = r->job.idx;
+            if (r->job.ntiles == 0) {  // no diagonal outside the exclusion zone
+                if (mpgpu::serve_finalize(r->job, st) != cudaSuccess) {
+                    cudaGetLastError();
+                    mpgpu::serve_release_result(r->job, st);
+                    r->d_d2 = nullptr;
+                    r->d_idx = nullptr;
+                    failed.push_back(r);
+                } else {
+                    finishing.push_back(r);
+                }
+                continue;
+            }
+            active.push_back(r);
+        }
+        if (!failed.empty()) {
+            cudaStreamSynchronize(st);
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                for (Request* r : failed) {
+                    r->d_d2 = nullptr;
+                    r->d_idx = nullptr;
+                }
+                complete_locked(s, failed, MP_ERR_OUT_OF_MEMORY);
+            }
+            s->cv_done.notify_all();
+        }
+        // one epoch over slices of every active request
+        std::vector<mpgpu::ServeSlice> slices = choose_slices(active);
+        if (!slices.empty()) {
+            mpgpu::serve_launch_epoch(eb, (int)(s->epochs_launched % mpgpu::ServeEpochBuffers::kRing),
+                                      slices, st);
+            ++s->epochs_launched;
+            for (const mpgpu::ServeSlice& sl : slices) sl.job->next_tile += sl.count;
+            for (auto it = active.begin(); it != active.end();) {
+                Request* r = *it;
+                if (r->job.next_tile >= r->job.ntiles) {
+                    mpgpu::serve_finalize(r->job, st);
+                    finishing.push_back(r);
+                    it = active.erase(it);
+                } else {
+                    ++it;
+                }
+            }
+        }
+        if (!finishing.empty() || !slices.empty()) {
+            cudaEvent_t ev;
+            if (!spare.empty()) {
+                ev = spare.back();
+                spare.pop_back();
+            } else {
+                cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            }
+            cudaEventRecord(ev, st);
+            inflight.push_back({ev, std::move(finishing)});
+        }
+        // keep kEpochsInFlight epochs queued; drain when there is nothing to add
+        while ((int)inflight.size() > kEpochsInFlight || (slices.empty() && !inflight.empty()))
+            retire_front();
+    }
+    while (!inflight.empty()) retire_front();
+    cudaStreamSynchronize(st);
+    for (cudaEvent_t e : spare) cudaEventDestroy(e);
+    mpgpu::serve_epoch_buffers_destroy(eb);
+    cudaStreamDestroy(st);
+}
+
 }  // namespace
 
 extern "C" {
@@ -163,7 +373,27 @@ int mp_server_create(int device, size_t mem_budget_bytes, int slots, int precisi
     s->precision = precision;
     s->reanchor_k = reanchor_k;
     s->free_slots = slots;
-    for (int i = 0; i < slots; ++i) s->workers.emplace_back(worker_main, s);
+    s->slots = slots;
+    s->epochs = precision == MP_PREC_FP32_REANCHOR;
+    if (s->epochs) {
+        // a pool of the server's own that keeps what it has been given (no
+        // release to the driver between requests); the budget bounds it
+        cudaSetDevice(device);
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            delete s;
+            return MP_ERR_CUDA;
+        }
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        s->engine = std::thread(engine_main, s);
+    } else {
+        for (int i = 0; i < slots; ++i) s->workers.emplace_back(worker_main, s);
+    }
     *out = s;
     return MP_OK;
 }
@@ -174,7 +404,8 @@ int mp_server_submit(mp_server* s, const double* A, int64_t n, int64_t m, int64_
     r->series.assign(A, A + n);
     r->m = m;
     r->PL = n - m + 1;
-    r->need = mp_selfjoin_scratch_bytes(n, m, s->precision) + result_bytes(n - m + 1);
+    r->need = s->epochs ? mpgpu::serve_scratch_bytes(n, m) + mpgpu::serve_result_bytes(n, m)
+                        : mp_selfjoin_scratch_bytes(n, m, s->precision) + result_bytes(n - m + 1);
     r->submitted = Clock::now();
     std::lock_guard<std::mutex> lk(s->mu);
     r->id = s->next_id++;
@@ -258,7 +489,7 @@ int mp_server_stats(mp_server* s, int64_t* completed, int64_t* rejected, int64_t
     if (completed) *completed = s->completed;
     if (rejected) *rejected = s->rejected;
     if (waiting) *waiting = (int64_t)s->waiting.size();
-    if (running) *running = (int64_t)s->workers.size() - s->free_slots;
+    if (running) *running = (int64_t)s->slots - s->free_slots;
     if (cells) *cells = s->cells_done;
     if (bytes_in_use) *bytes_in_use = s->in_use;
     return MP_OK;
@@ -273,11 +504,17 @@ int mp_server_destroy(mp_server* s) {
     }
     s->cv_work.notify_all();
     for (auto& t : s->workers) t.join();
+    if (s->engine.joinable()) s->engine.join();
     cudaSetDevice(s->device);
+    cudaStream_t st;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     for (auto& kv : s->reqs) {
-        if (kv.second->d_d2) cudaFree(kv.second->d_d2);
-        if (kv.second->d_idx) cudaFree(kv.second->d_idx);
+        if (kv.second->d_d2) cudaFreeAsync(kv.second->d_d2, st);
+        if (kv.second->d_idx) cudaFreeAsync(kv.second->d_idx, st);
     }
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
     return MP_OK;
 }

@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(128) fp64_guard_kernel(const Fp32TileParams* _
         const Fp32TileParams P = series[lo];
         if (!P.hazard) continue;
         int64_t band, seg;
-        if (fp32_tile_of(P, tt - P.tile_begin, 32 * R, band, seg)) tile_guard<R>(P, band, seg, lane);
+        if (fp32_tile_of(P, tt - P.tile_begin + P.tile_skip, 32 * R, band, seg)) tile_guard<R>(P, band, seg, lane);
     }
 }
 

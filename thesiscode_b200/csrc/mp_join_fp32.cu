@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(32 * kFp32WarpsPerBlock, MPGPU_FP32_MIN_BLOCKS
         // tile counts); consecutive tiles are consecutive column segments of
         // one band, so tiles running together touch disjoint columns and rows
         int64_t band, seg;
-        if (fp32_tile_of(P, tt - P.tile_begin, 32 * R, band, seg))
+        if (fp32_tile_of(P, tt - P.tile_begin + P.tile_skip, 32 * R, band, seg))
             tile_fp32<R>(P, band, seg, lane, ring, rring, cring);
     }
 }

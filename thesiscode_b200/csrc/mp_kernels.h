@@ -87,7 +87,9 @@ void launch_fp64_band(const Fp64BandParams& P, cudaStream_t s);
 
 // ---- FP32 re-anchored tile join (mp_join_fp32.cu) ---------------------------
 // One series of a (batched) join.  Its tiles are numbered
-// [tile_begin, tile_begin + npairs * seg_per_pair) in the launch's tile space.
+// [tile_begin, tile_begin + npairs * seg_per_pair) in the launch's tile space;
+// a launch that runs only a slice of them (the request server's epochs) starts
+// at the series' local tile tile_skip.
 struct Fp32TileParams {
     const float4* rowrec;  // pairs (x[j], x[j+H]) of df, dg, nn; 2 float4 per row
     const float4* colrec;  // duplicated, negated column terms; 2 float4 per column
@@ -99,6 +101,7 @@ struct Fp32TileParams {
     int64_t nbands;        // bands of 32R diagonals
     int64_t seg_per_pair;  // tiles per band pair (k, nbands-1-k), max over pairs
     int64_t tile_begin;    // first tile of this series in the launch
+    int64_t tile_skip;     // local tile that launch tile tile_begin stands for (0: all)
     unsigned long long* key;  // [PL] (ordered u << 32 | neighbour), min-merged
     // Guarded form only (all null otherwise): hazard[w] = number of hazard
     // windows among [0, w) (PL + 1 entries); FP64 inverse norms and

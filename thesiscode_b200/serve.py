@@ -44,13 +44,13 @@ def _producer(reqs, out: queue.Queue, stop: threading.Event):
             return
 
 
-def run_stream(rate: float, duration: float, slots: int = 4, budget_gb: float = 64.0,
+def run_stream(rate: float, duration: float, slots: int = 32, budget_gb: float = 64.0,
                seed: int = 4, max_n: int | None = None, drain_timeout: float = 120.0,
                server=None, lookahead: int = 32, servers=None, devices=None):
     """Replays the c5 stream at `rate`.  Requests go round-robin to `servers`
     (objects with submit/done/collect/stats/close), or to `server`, or to new
-    mp.Server replicas on `devices` (default: device 0), `slots` workers and
-    `budget_gb` of device memory each."""
+    mp.Server replicas on `devices` (default: device 0), each admitting at most
+    `slots` requests at once within `budget_gb` of device memory."""
     reqs = workloads.c5_stream(rate, duration, seed)
     if max_n:
         reqs = [(t, min(n, max_n), m, s) for t, n, m, s in reqs]
@@ -154,7 +154,7 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--rate", type=float, nargs="+", default=[10, 30, 100])
     ap.add_argument("--duration", type=float, default=10.0)
-    ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--slots", type=int, default=32)
     ap.add_argument("--budget-gb", type=float, default=64.0)
     ap.add_argument("--gpus", type=int, default=1, help="replicas, one server per GPU")
     a = ap.parse_args()
