@@ -14,8 +14,9 @@ on the stream the library launches on; an L2 flush (256 MB write) runs between
 steps outside the events; barrier + device synchronisation around the loop;
 the maximum over ranks is reported.  With N > 1 the diagonals are split into
 2N partitions, rank r taking partitions r and 2N-1-r (the reference's
-scrimp_triv_par balance rule), and the partial profiles are merged with one
-NCCL all-gather plus an element-wise arg-min.
+scrimp_triv_par balance rule) in one mp_selfjoin_ranges call, and the partial
+profiles are merged with NCCL MIN all-reduces of packed keys (one for the
+FP32 form, two for the FP64 form; shard.allreduce_profiles).
 
 --impl reference times the reference's own CPU code (oracle/_ref, built from
 its unchanged sources; else the C restatement) on all host cores, each step a
@@ -218,28 +219,15 @@ def run_ours(args, world):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
 
     def one_step(precision):
-        launches = 0
-        join_ms = 0.0
-        first = True
-        for a, b in mine:
-            tgt = (d2, ix) if first else (d2b, ixb)
-            ctx.selfjoin(xd, m, precision=precision, reanchor_k=args.reanchor_k, diag_lo=a,
-                         diag_hi=b, out=tgt, stream=stream.cuda_stream)
-            launches += ctx.last_launch_count
-            join_ms += ctx.last_phase_ms()[1]
-            if not first:
-                with torch.cuda.stream(stream):
-                    md, mi = shard.merge_profiles([d2, d2b], [ix, ixb])
-                    d2.copy_(md)
-                    ix.copy_(mi)
-            first = False
+        # one call over this rank's diagonal partitions (one preparation, one
+        # sync), then, with N > 1, the MIN all-reduce of packed keys
+        ctx.selfjoin_ranges(xd, m, mine, precision=precision, reanchor_k=args.reanchor_k,
+                            out=(d2, ix), stream=stream.cuda_stream)
+        launches = ctx.last_launch_count
+        join_ms = ctx.last_phase_ms()[1]
         if world > 1:
             with torch.cuda.stream(stream):
-                gd = [torch.empty_like(d2) for _ in range(world)]
-                gi = [torch.empty_like(ix) for _ in range(world)]
-                dist.all_gather(gd, d2)
-                dist.all_gather(gi, ix)
-                md, mi = shard.merge_profiles(gd, gi)
+                md, mi = shard.allreduce_profiles(d2, ix, m, fp32_form=precision != mp.FP64)
                 d2.copy_(md)
                 ix.copy_(mi)
         return launches, join_ms
@@ -295,15 +283,16 @@ def run_ours(args, world):
 
     # -- end to end with pinned host buffers ----------------------------------------
     # N = 1: one mp_selfjoin call on host pointers (it copies in and out itself).
-    # N > 1: every rank copies the series in, joins its diagonal partitions and
-    # merges through one all-gather (shard.distributed_selfjoin); rank 0 reads
-    # the profile back.  Timed per rank with CUDA events, max over ranks.
+    # N > 1: every rank copies the series in, joins its diagonal partitions in
+    # one call and merges through one MIN all-reduce (shard.distributed_selfjoin);
+    # rank 0 reads the profile back.  Timed per rank with CUDA events, max over
+    # ranks.
     xh = torch.from_numpy(x).pin_memory()
     oh = (torch.empty(PL, dtype=torch.float64).pin_memory(),
           torch.empty(PL, dtype=torch.int64).pin_memory())
     xdev = torch.empty(n, dtype=torch.float64, device=dev)
-    parts = [(torch.empty(PL, dtype=torch.float64, device=dev),
-              torch.empty(PL, dtype=torch.int64, device=dev)) for _ in range(2)]
+    parts = (torch.empty(PL, dtype=torch.float64, device=dev),
+             torch.empty(PL, dtype=torch.int64, device=dev))
 
     def e2e_step():
         if world == 1:
@@ -312,17 +301,15 @@ def run_ours(args, world):
             return
         with torch.cuda.stream(stream):
             xdev.copy_(xh, non_blocking=True)
-        used = [0]
 
-        def compute(a, b):
-            d, i = parts[used[0]]
-            used[0] += 1
-            ctx.selfjoin(xdev, m, precision=mp.FP32_REANCHOR, reanchor_k=args.reanchor_k,
-                         diag_lo=a, diag_hi=b, out=(d, i), stream=stream.cuda_stream)
+        def compute(ranges):
+            d, i = parts
+            ctx.selfjoin_ranges(xdev, m, ranges, precision=mp.FP32_REANCHOR,
+                                reanchor_k=args.reanchor_k, out=(d, i), stream=stream.cuda_stream)
             return d, i
 
         with torch.cuda.stream(stream):
-            md, mi = shard.distributed_selfjoin(compute, n, m)
+            md, mi = shard.distributed_selfjoin(compute, n, m, fp32_form=True)
             if rank == 0:
                 oh[0].copy_(md, non_blocking=True)
                 oh[1].copy_(mi, non_blocking=True)
@@ -351,8 +338,10 @@ def run_ours(args, world):
     e2e = {"value": cells_total * len(lat) / (tot_e2e * 1e-3), "unit": "cells/s",
            "h2d_bytes_per_step": 8 * n * world, "d2h_bytes_per_step": 16 * PL,
            "path": "mp_selfjoin (C ABI) with pinned host input/outputs" if world == 1 else
-           f"pinned host series to each of {world} GPUs, mp_selfjoin per diagonal partition, "
-           "NCCL all-gather merge (shard.distributed_selfjoin), profile to pinned host on rank 0"}
+           f"pinned host series to each of {world} GPUs, one mp_selfjoin_ranges call over the "
+           "rank's two diagonal partitions, "
+           "NCCL MIN all-reduce of packed keys (shard.distributed_selfjoin), profile to pinned host "
+           "on rank 0"}
 
     # the FP64 form's phases on one more (untimed) call: preparation holds the
     # reference-order statistics and the first dot products of every diagonal
@@ -409,7 +398,7 @@ def run_ours(args, world):
                    "n": n, "m": m, "reanchor_k": args.reanchor_k, "cells": cells_total,
                    "l2": f"flushed between steps (256 MB write); working set "
                          f"~{(8 * n + 80 * PL) / 1e6:.0f} MB",
-                   "parallelism": f"diagonal partitions x{2 * world}, NCCL all-gather merge"
+                   "parallelism": f"diagonal partitions x{2 * world}, NCCL MIN all-reduce merge"
                    if world > 1 else "single GPU"},
         "fp64_baseline": {"value": value64, "unit": "cells/s", "ms_per_step": tot64 / fsteps,
                           "kernel": "fp64_band_kernel (reference arithmetic, bit-identical)",

@@ -98,6 +98,19 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
                 int64_t diag_hi, double* dist2_out, int64_t* idx_out, void* stream);
 
 /*
+ * mp_selfjoin over several diagonal ranges at once: ranges[2i], ranges[2i+1]
+ * are the bounds [lo, hi) of range i (clipped to excl+1 .. PL-1; empty ones are
+ * skipped).  One preparation, every range joined into the same profile, one
+ * finalisation and one synchronisation -- the per-rank part of a join sharded
+ * by the reference's scrimp_triv_par rule, where rank r of P evaluates
+ * partitions r and 2P-1-r (scrimppp/src/ScrimpTrivialPar.cpp:200-224).  The
+ * guarded form takes one range only (MP_ERR_NOT_SUPPORTED otherwise).
+ */
+int mp_selfjoin_ranges(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t excl,
+                       int precision, int64_t reanchor_k, int64_t blocklen, const int64_t* ranges,
+                       int64_t count, double* dist2_out, int64_t* idx_out, void* stream);
+
+/*
  * One block of diagonals, the reference's kernel interface
  * (scrimppp/inc/kernels.h:7-24, scrimppp/src/kernels.cpp:368-410), evaluated
  * on the GPU in FP64 with the reference's per-cell arithmetic.  Arguments have

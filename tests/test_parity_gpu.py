@@ -227,3 +227,32 @@ def test_errors_are_status_codes(gpu_ctx):
         small.selfjoin(workloads.random_walk(100000, 1), 64)
     assert e.value.status == mp.MP_ERR_BUDGET
     small.close()
+
+
+def test_selfjoin_ranges_one_call_equals_separate_calls(gpu_ctx, oracle):
+    """A rank's two diagonal partitions (the reference's triv_par rule) in one
+    mp_selfjoin_ranges call give the element-wise arg-min of the two separate
+    joins; the FP64 form stays bit-identical to the oracle on those ranges."""
+    from thesiscode_b200 import shard
+    x = workloads.random_walk(20000, 31)
+    m = 64
+    for rank in (0, 1):
+        ranges = shard.rank_ranges(x.size, m, rank, 2)
+        assert len(ranges) == 2
+        for prec in (mp.FP64, mp.FP32_REANCHOR):
+            one = gpu_ctx.selfjoin_ranges(x, m, ranges, precision=prec, reanchor_k=256)
+            parts = [gpu_ctx.selfjoin(x, m, precision=prec, reanchor_k=256, diag_lo=a, diag_hi=b)
+                     for a, b in ranges]
+            md, mi = shard.merge_profiles([p.dist2 for p in parts], [p.index for p in parts])
+            assert np.array_equal(one.dist2, md), (rank, prec)
+            if prec == mp.FP32_REANCHOR:
+                assert np.array_equal(one.index, mi), rank
+            else:
+                refs = [oracle.selfjoin(x, m, diag_lo=a, diag_hi=b) for a, b in ranges]
+                rd, ri = shard.merge_profiles([r[0] for r in refs], [r[1] for r in refs])
+                assert np.array_equal(one.dist2, rd), rank
+                check_fp64_indices(oracle, x, m, one.dist2, one.index, ri)
+    with pytest.raises(mp.MpError) as e:
+        gpu_ctx.selfjoin_ranges(x, m, shard.rank_ranges(x.size, m, 0, 2),
+                                precision=mp.FP32_GUARDED)
+    assert e.value.status == mp.MP_ERR_NOT_SUPPORTED

@@ -1,6 +1,8 @@
 """Diagonal sharding across ranks (the multi-GPU path) on CPU: world-size-2
-gloo process groups, per-rank partial profiles from the oracle, one
-all-gather merge; the merged profile must equal the single-process join."""
+gloo process groups, per-rank partial profiles from the oracle, merged by
+MIN all-reduces of packed keys; the merged profile must equal the
+single-process join (FP64 form) or the element-wise arg-min of the partial
+profiles (FP32 form)."""
 from __future__ import annotations
 
 import os
@@ -61,8 +63,9 @@ def _worker(rank, world, port, n, m, q):
         x = workloads.random_walk(n, 5)
         orc = Oracle()
 
-        def compute(lo, hi):
-            d2, ix = orc.selfjoin(x, m, diag_lo=lo, diag_hi=hi, nthreads=1)
+        def compute(ranges):
+            parts = [orc.selfjoin(x, m, diag_lo=lo, diag_hi=hi, nthreads=1) for lo, hi in ranges]
+            d2, ix = shard.merge_profiles([p[0] for p in parts], [p[1] for p in parts])
             return torch.from_numpy(d2), torch.from_numpy(ix)
 
         d2, ix = shard.distributed_selfjoin(compute, n, m)
@@ -103,11 +106,13 @@ def _failing_worker(rank, world, port, bad_rank, q):
         n, m = 3000, 32
         x = workloads.random_walk(n, 9)
 
-        def compute(lo, hi):
+        def compute(ranges):
             if rank == bad_rank:
                 raise RuntimeError("device scratch allocation failed")
             from oracle.oracle import Oracle
-            d2, ix = Oracle().selfjoin(x, m, diag_lo=lo, diag_hi=hi, nthreads=1)
+            parts = [Oracle().selfjoin(x, m, diag_lo=lo, diag_hi=hi, nthreads=1)
+                     for lo, hi in ranges]
+            d2, ix = shard.merge_profiles([p[0] for p in parts], [p[1] for p in parts])
             return torch.from_numpy(d2), torch.from_numpy(ix)
 
         try:
@@ -141,6 +146,64 @@ def test_failed_rank_is_reported_on_every_rank(oracle, bad_rank):
     assert res == [(r, "ShardFailure", [bad_rank]) for r in range(world)]
     assert all(p.exitcode == 0 for p in procs)
 
+
+
+def _fp32_partial(seed, PL, m):
+    """A synthetic FP32-form partial profile: d2 = 2m * u with u an FP32 value,
+    some windows without a neighbour (2m + 2, index 0), some exact ties."""
+    rng = np.random.default_rng(seed)
+    u = rng.uniform(0.0, 1.0, PL).astype(np.float32)
+    u[::7] = np.float32(0.25)  # equal distances across ranks: the index decides
+    d2 = 2.0 * m * u.astype(np.float64)
+    ix = rng.integers(0, PL, PL).astype(np.int64)
+    none = rng.random(PL) < 0.1
+    d2[none], ix[none] = 2.0 * m + 2.0, 0
+    return d2, ix
+
+
+def test_fp32_keys_round_trip_and_order():
+    m, PL = 96, 5000
+    d2, ix = _fp32_partial(3, PL, m)
+    # zero, below zero (u < 0 by rounding), tiny: all 2m times an FP32 value
+    d2[:3] = 2.0 * m * np.array([0.0, -1e-7, 1e-30], dtype=np.float32).astype(np.float64)
+    key = shard.pack_fp32_keys(torch.from_numpy(d2), torch.from_numpy(ix), m)
+    back_d2, back_ix = shard.unpack_fp32_keys(key, m)
+    assert np.array_equal(back_d2.numpy(), d2) and np.array_equal(back_ix.numpy(), ix)
+    order = np.lexsort((ix, d2))
+    assert np.all(np.diff(key.numpy()[order]) >= 0)
+
+
+def _fp32_merge_worker(rank, world, port, m, PL, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        d2, ix = _fp32_partial(40 + rank, PL, m)
+        md, mi = shard.allreduce_profiles(torch.from_numpy(d2), torch.from_numpy(ix), m,
+                                          fp32_form=True)
+        q.put((rank, md.numpy(), mi.numpy()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_fp32_allreduce_equals_argmin_merge():
+    world, m, PL = 2, 128, 3000
+    ctx = tmp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_fp32_merge_worker, args=(r, world, port, m, PL, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    parts = [_fp32_partial(40 + r, PL, m) for r in range(world)]
+    want_d2, want_ix = shard.merge_profiles([p[0] for p in parts], [p[1] for p in parts])
+    for rank, d2, ix in res:
+        assert np.array_equal(d2, want_d2), rank
+        assert np.array_equal(ix, want_ix), rank
 
 
 def test_balance_by_cost_for_batch_replicas():

@@ -51,7 +51,7 @@ EXPORTED_SYMBOLS = (
     "mp_batch_launch_count", "mp_batch_upload", "mp_batch_launch", "mp_batch_download",
     "mp_batch_run", "mp_server_create", "mp_server_submit", "mp_server_poll", "mp_server_collect",
     "mp_server_stats", "mp_server_destroy", "mp_selfjoin_fp32_noalloc", "mp_prescrimp",
-    "mp_last_near_duplicates",
+    "mp_last_near_duplicates", "mp_selfjoin_ranges",
 )
 
 
@@ -85,6 +85,8 @@ def load_library() -> ctypes.CDLL:
     L.mp_selfjoin_scratch_bytes.restype = ctypes.c_size_t
     L.mp_selfjoin.argtypes = [_P, _P, _i64, _i64, _i64, ctypes.c_int, _i64, _i64, _i64, _i64,
                               _P, _P, _P]
+    L.mp_selfjoin_ranges.argtypes = [_P, _P, _i64, _i64, _i64, ctypes.c_int, _i64, _i64, _P,
+                                     _i64, _P, _P, _P]
     L.mp_eval_diag_block_triangle.argtypes = [_P, _P, _P, _P, _P, _P, _i64, _i64, _P, _P, _i64,
                                               _P, _P, _P, _P, _i64, _i64, _P]
     L.mp_window_stats.argtypes = [_P, _P, _i64, _i64, _P, _P, _P]
@@ -250,6 +252,28 @@ class Context:
             d2, ix = out
         rc = self._L.mp_selfjoin(self._h, _ptr(A), n, m, excl, precision, reanchor_k, blocklen,
                                  diag_lo, diag_hi, _ptr(d2), _ptr(ix), stream)
+        self._check(rc)
+        return Profile(d2, ix)
+
+    def selfjoin_ranges(self, A, m: int, ranges, precision: int = FP64, reanchor_k: int = 0,
+                        blocklen: int = 0, excl: int = -1, out=None, stream=None) -> Profile:
+        """selfjoin over several diagonal ranges [(lo, hi), ...] in one call (one
+        preparation and one synchronisation): a rank's part of a sharded join."""
+        if isinstance(A, np.ndarray):
+            A = np.ascontiguousarray(A, dtype=np.float64)
+            n = A.size
+        else:
+            n = A.numel()
+        PL = n - m + 1
+        if out is None:
+            d2 = np.empty(max(PL, 0), dtype=np.float64)
+            ix = np.empty(max(PL, 0), dtype=np.int64)
+        else:
+            d2, ix = out
+        flat = np.ascontiguousarray(np.asarray(ranges, dtype=np.int64).reshape(-1))
+        rc = self._L.mp_selfjoin_ranges(self._h, _ptr(A), n, m, excl, precision, reanchor_k,
+                                        blocklen, flat.ctypes.data if flat.size else None,
+                                        flat.size // 2, _ptr(d2), _ptr(ix), stream)
         self._check(rc)
         return Profile(d2, ix)
 

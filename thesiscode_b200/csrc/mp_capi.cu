@@ -206,7 +206,7 @@ size_t guard_scratch(int64_t n, int64_t m) {
            4 * align_up(8 * (size_t)PL) + align_up(4 * (size_t)kNearDupCap) + 2048;
 }
 
-size_t fp32_scratch(int64_t n, int64_t m, bool host_io) {
+size_t fp32_scratch(int64_t n, int64_t m, bool host_io, size_t nranges = 1) {
     const int64_t PL = n - m + 1;
     size_t b = 0;
     b += align_up(8 * (size_t)(n + kFp32Pad));   // Apad
@@ -215,7 +215,7 @@ size_t fp32_scratch(int64_t n, int64_t m, bool host_io) {
     b += 2 * align_up(8 * (size_t)(PL + kFp32Pad));  // mean, norm
     b += 2 * align_up(32 * (size_t)(PL + kFp32Pad)); // row/col records
     b += align_up(8 * (size_t)PL);               // keys
-    b += align_up(sizeof(Fp32TileParams)) + 256; // descriptor, tile counter
+    b += align_up(sizeof(Fp32TileParams) * std::max<size_t>(nranges, 1)) + 256;  // descriptors, tile counter
     if (host_io) b += align_up(8 * (size_t)PL) * 2;
     return b + 4096;
 }
@@ -314,12 +314,22 @@ size_t mp_selfjoin_scratch_bytes(int64_t n, int64_t m, int precision) {
     return fp32_scratch(n, m, true);
 }
 
-int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t excl,
-                int precision, int64_t reanchor_k, int64_t blocklen, int64_t diag_lo,
-                int64_t diag_hi, double* dist2_out, int64_t* idx_out, void* stream) {
-    Sizes S;
-    int rc = check_join_args(ctx, A, n, m, excl, diag_lo, diag_hi, dist2_out, idx_out, S);
-    if (rc) return rc;
+}  // extern "C"
+
+namespace {
+
+struct DiagRange {
+    int64_t lo, hi;
+};
+
+// The self-join over a list of non-empty diagonal ranges [lo, hi) inside
+// [S.lo, S.hi): one preparation, the joins of every range into the same keys,
+// one finalisation.
+int selfjoin_ranges(mp_context* ctx, const double* A, int64_t n, int64_t m, int precision,
+                    int64_t reanchor_k, int64_t blocklen, const Sizes& S,
+                    const std::vector<DiagRange>& ranges, double* dist2_out, int64_t* idx_out,
+                    void* stream) {
+    int rc = MP_OK;
     if (precision != MP_PREC_FP64 && precision != MP_PREC_FP32_REANCHOR &&
         precision != MP_PREC_FP32_GUARDED)
         return fail(ctx, MP_ERR_INVALID_ARG, "unknown precision %d", precision);
@@ -337,7 +347,11 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
     const bool o_dev = sd == MemSpace::Device;
     if ((si == MemSpace::Device) != o_dev)
         return fail(ctx, MP_ERR_INVALID_ARG, "dist2_out and idx_out live in different memory spaces");
-    const int64_t PL = S.PL, ndiag = S.hi - S.lo;
+    const int64_t PL = S.PL;
+    int64_t ndiag = 0;
+    for (const DiagRange& r : ranges) ndiag += r.hi - r.lo;
+    if (precision == MP_PREC_FP32_GUARDED && ranges.size() > 1)
+        return fail(ctx, MP_ERR_NOT_SUPPORTED, "the guarded form takes one diagonal range per call");
 
     if (precision == MP_PREC_FP64) {
         const int64_t B = blocklen > 0 ? blocklen : 500;
@@ -366,9 +380,14 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
         MP_LAUNCHED(ctx);
         ref_stats_kernel<<<grid_for(PL), kThreads, 0, st>>>(cs, cs2, PL, m, muS, sInv);
         MP_LAUNCHED(ctx);
-        if (ndiag > 0) {
-            first_qt_kernel<<<grid_for(ndiag), kThreads, 0, st>>>(Apad, m, S.lo, S.hi, qt0);
-            MP_LAUNCHED(ctx);
+        {
+            int64_t off = 0;
+            for (const DiagRange& r : ranges) {
+                first_qt_kernel<<<grid_for(r.hi - r.lo), kThreads, 0, st>>>(Apad, m, r.lo, r.hi,
+                                                                          qt0 + off);
+                MP_LAUNCHED(ctx);
+                off += r.hi - r.lo;
+            }
         }
         MP_CUDA(ctx, cudaMemsetAsync(rec + PL, 0, 32 * kFp64Pad, st));
         pack_fp64_kernel<<<grid_for(PL), kThreads, 0, st>>>(Apad, m, PL, sInv, muS, rec);
@@ -379,16 +398,19 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
             reinterpret_cast<unsigned long long*>(thr), PL + kFp64ThrPad, no_threshold_bits());
         MP_LAUNCHED(ctx);
         mark(ctx, 1, st);
-        if (ndiag > 0) {
+        int64_t qoff = 0;
+        for (const DiagRange& r : ranges) {
             Fp64BandParams P{};
-            const int R = pick_fp64_R(ndiag);
+            const int64_t nd = r.hi - r.lo;
+            const int R = pick_fp64_R(nd);
             P.colrec = rec;
             P.rowrec = rec;
-            P.qt0 = qt0;
+            P.qt0 = qt0 + qoff;
+            qoff += nd;
             P.qt_out = nullptr;
-            P.g_lo = S.lo;
-            P.g_hi = S.hi;
-            P.nbands = (ndiag + 32 * R - 1) / (32 * R);
+            P.g_lo = r.lo;
+            P.g_hi = r.hi;
+            P.nbands = (nd + 32 * R - 1) / (32 * R);
             P.blk_origin = S.excl + 1;
             P.B = B;
             P.Tbase = PL;
@@ -423,7 +445,7 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
     // ---- FP32 re-anchored form ----------------------------------------------
     const int64_t K = reanchor_interval(reanchor_k, kFp32R);
     const bool guarded = precision == MP_PREC_FP32_GUARDED;
-    rc = reserve(ctx, fp32_scratch(n, m, !o_dev) + (guarded ? guard_scratch(n, m) : 0));
+    rc = reserve(ctx, fp32_scratch(n, m, !o_dev, ranges.size()) + (guarded ? guard_scratch(n, m) : 0));
     if (rc) return rc;
     Carve cv{(char*)ctx->arena};
     double* Apad = cv.take<double>(n + kFp32Pad);
@@ -435,7 +457,7 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
     float4* rowrec = cv.take<float4>(2 * (PL + kFp32Pad));
     float4* colrec = cv.take<float4>(2 * (PL + kFp32Pad));
     unsigned long long* key = cv.take<unsigned long long>(PL);
-    Fp32TileParams* desc = cv.take<Fp32TileParams>(1);
+    Fp32TileParams* desc = cv.take<Fp32TileParams>(std::max<int64_t>((int64_t)ranges.size(), 1));
     unsigned long long* counter = cv.take<unsigned long long>(1);
     double* d2 = o_dev ? dist2_out : cv.take<double>(PL);
     int64_t* ix = o_dev ? idx_out : cv.take<int64_t>(PL);
@@ -467,20 +489,28 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
     MP_LAUNCHED(ctx);
     mark(ctx, 1, st);
     if (ndiag > 0) {
-        Fp32TileParams P{};
-        P.rowrec = rowrec;
-        P.colrec = colrec;
-        P.A = Apad;
-        P.mean = mean;
-        P.m = m;
-        P.PL = PL;
-        P.g_lo = S.lo;
-        P.g_hi = S.hi;
-        P.K = K;
+        // one descriptor per diagonal range, all merging into the same keys
+        std::vector<Fp32TileParams> Ps;
         int64_t ntiles = 0;
-        fp32_tile_plan(PL, S.lo, S.hi, K, kFp32R, P.nbands, P.seg_per_pair, ntiles);
-        P.tile_begin = 0;
-        P.key = key;
+        for (const DiagRange& r : ranges) {
+            Fp32TileParams Q{};
+            Q.rowrec = rowrec;
+            Q.colrec = colrec;
+            Q.A = Apad;
+            Q.mean = mean;
+            Q.m = m;
+            Q.PL = PL;
+            Q.g_lo = r.lo;
+            Q.g_hi = r.hi;
+            Q.K = K;
+            int64_t nt = 0;
+            fp32_tile_plan(PL, r.lo, r.hi, K, kFp32R, Q.nbands, Q.seg_per_pair, nt);
+            Q.tile_begin = ntiles;
+            ntiles += nt;
+            Q.key = key;
+            Ps.push_back(Q);
+        }
+        Fp32TileParams& P = Ps[0];  // the guarded form has exactly one range
         if (guarded) {
             // hazard windows (prefix counts over PL + 1 entries) and FP64 terms
             int* hz = cv.take<int>(PL + 1);
@@ -510,9 +540,10 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
             P.df = gdf;
             P.dg = gdg;
         }
-        MP_CUDA(ctx, cudaMemcpyAsync(desc, &P, sizeof P, cudaMemcpyHostToDevice, st));
+        MP_CUDA(ctx, cudaMemcpyAsync(desc, Ps.data(), sizeof(Fp32TileParams) * Ps.size(),
+                                     cudaMemcpyHostToDevice, st));
         MP_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
-        launch_fp32_join<kFp32R>(desc, 1, ntiles, counter, st);
+        launch_fp32_join<kFp32R>(desc, (int)Ps.size(), ntiles, counter, st);
         MP_LAUNCHED(ctx);
         if (guarded) {
             // the same tiles again: the FP64 pass evaluates those the FP32 pass skipped
@@ -540,8 +571,8 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
                 N.norm = norm;
                 N.m = m;
                 N.PL = PL;
-                N.g_lo = S.lo;
-                N.g_hi = S.hi;
+                N.g_lo = P.g_lo;
+                N.g_hi = P.g_hi;
                 N.list = ndl;
                 N.count = nd;
                 N.key = key;
@@ -567,6 +598,41 @@ int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t 
     MP_CUDA(ctx, cudaStreamSynchronize(st));
     collect_phases(ctx);
     return MP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mp_selfjoin(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t excl,
+                int precision, int64_t reanchor_k, int64_t blocklen, int64_t diag_lo,
+                int64_t diag_hi, double* dist2_out, int64_t* idx_out, void* stream) {
+    Sizes S;
+    int rc = check_join_args(ctx, A, n, m, excl, diag_lo, diag_hi, dist2_out, idx_out, S);
+    if (rc) return rc;
+    std::vector<DiagRange> ranges;
+    if (S.hi > S.lo) ranges.push_back({S.lo, S.hi});
+    return selfjoin_ranges(ctx, A, n, m, precision, reanchor_k, blocklen, S, ranges, dist2_out,
+                           idx_out, stream);
+}
+
+int mp_selfjoin_ranges(mp_context* ctx, const double* A, int64_t n, int64_t m, int64_t excl,
+                       int precision, int64_t reanchor_k, int64_t blocklen, const int64_t* ranges,
+                       int64_t count, double* dist2_out, int64_t* idx_out, void* stream) {
+    Sizes S;
+    int rc = check_join_args(ctx, A, n, m, excl, 0, 0, dist2_out, idx_out, S);
+    if (rc) return rc;
+    if (count < 0 || (count > 0 && !ranges))
+        return fail(ctx, MP_ERR_INVALID_ARG, "bad diagonal range list");
+    std::vector<DiagRange> list;
+    for (int64_t i = 0; i < count; ++i) {
+        if (ranges[2 * i] > ranges[2 * i + 1])
+            return fail(ctx, MP_ERR_INVALID_ARG, "diagonal range %lld has lo > hi", (long long)i);
+        const int64_t lo = std::max(ranges[2 * i], S.lo), hi = std::min(ranges[2 * i + 1], S.hi);
+        if (hi > lo) list.push_back({lo, hi});
+    }
+    return selfjoin_ranges(ctx, A, n, m, precision, reanchor_k, blocklen, S, list, dist2_out,
+                           idx_out, stream);
 }
 
 int mp_window_stats(mp_context* ctx, const double* A, int64_t n, int64_t m, double* muS_out,
