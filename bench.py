@@ -47,6 +47,19 @@ def host_cores() -> int:
         return os.cpu_count() or 1
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (from /proc/cpuinfo), or the platform's."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.lower().startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or platform.machine()
+
+
 def sample_range(n: int, m: int, target_cells: float):
     """Diagonal range [excl+1, hi) holding about target_cells cells."""
     PL, lo = n - m + 1, m // 4 + 1
@@ -154,6 +167,117 @@ def cpu_reference_run(x, m, target_seconds: float, threads: int):
     return cells, sec, kind, sample
 
 
+def parity_checks(ctx, workload, x, m, d2_64, idx_64, d2_32):
+    """This run's GPU results against the reference, outside the timed region.
+
+    - digest: SHA-256 of the FP64 form's squared distances (and indices) against
+      the digests tests/golden/make_golden.py recorded from the reference's own
+      code for this workload (c1, c2);
+    - index_sample: for a seeded sample of windows, the reference's own score of
+      the cell (window, chosen neighbour), recomputed on the host with the
+      reference's per-cell arithmetic, gives exactly the FP64 form's squared
+      distance (so the neighbour attains the profile value; a different index
+      in the reference can only be an exact tie);
+    - fp32_vs_fp64: the FP32 form's relative distance error against that FP64
+      profile (the bound is 1e-4);
+    - test_ascii: the FP64 form on the reference's own fixture
+      (data_testing/test.ascii, m in {16, 64, 400}) against its golden profiles,
+      bit for bit, indices by the same tie rule.
+    """
+    import hashlib
+
+    import thesiscode_b200 as mp
+    from oracle.oracle import Oracle
+    golden = os.path.join(ROOT, "tests", "golden")
+    orc = Oracle()
+    out = {}
+    digests = json.load(open(os.path.join(golden, "digests.json")))
+    if workload in digests:
+        want = digests[workload]
+        out["digest"] = {
+            "workload": workload,
+            "d2_sha256_match": hashlib.sha256(d2_64.tobytes()).hexdigest() == want["d2_sha256"],
+            "idx_sha256_match": hashlib.sha256(idx_64.tobytes()).hexdigest() == want["idx_sha256"],
+        }
+
+    def neighbour_attains(xs, mm, d2, idx, wins):
+        stats = orc.window_stats(xs, mm)
+        valid = [i for i in wins if not (d2[i] == 2 * mm + 2 and idx[i] == 0)]
+        if not valid:
+            return 0, 0
+        i = np.asarray(valid, dtype=np.int64)
+        j = idx[i]
+        s = orc.cell_scores(xs, mm, np.minimum(i, j), np.maximum(i, j), 500, stats=stats)
+        return int(np.sum(2.0 * mm - 2.0 * s != d2[i])), len(valid)
+
+    rng = np.random.default_rng(7)
+    PL = x.size - m + 1
+    wins = rng.choice(PL, size=min(256, PL), replace=False)
+    bad, checked = neighbour_attains(x, m, d2_64, idx_64, wins)
+    out["index_sample"] = {"windows": checked, "neighbour_not_attaining_value": bad}
+    dt = np.sqrt(np.abs(d2_64))
+    rel = np.abs(np.sqrt(np.abs(d2_32)) - dt) / dt
+    out["fp32_vs_fp64"] = {"max_rel": float(rel.max()), "mean_rel": float(rel.mean()),
+                           "bound": 1e-4, "within": bool(rel.max() <= 1e-4)}
+    ga = np.load(os.path.join(golden, "test_ascii.npz"))
+    series = ga["series"]
+    ta = {}
+    for mm in (16, 64, 400):
+        p = ctx.selfjoin(series, mm, precision=mp.FP64)
+        diff = np.nonzero(p.index != ga[f"idx_m{mm}"])[0]
+        ties = 0
+        if diff.size:
+            stats = orc.window_stats(series, mm)
+            a, b = p.index[diff], ga[f"idx_m{mm}"][diff]
+            sa = orc.cell_scores(series, mm, np.minimum(diff, a), np.maximum(diff, a), 500,
+                                 stats=stats)
+            sb = orc.cell_scores(series, mm, np.minimum(diff, b), np.maximum(diff, b), 500,
+                                 stats=stats)
+            da, db = np.sqrt(np.abs(2.0 * mm - 2.0 * sa)), np.sqrt(np.abs(2.0 * mm - 2.0 * sb))
+            ties = int(np.sum((sa == sb) | (np.abs(da - db) <= 1e-9 * db)))
+        ta[f"m{mm}"] = {"d2_bit_identical": bool(np.array_equal(p.dist2, ga[f"d2_m{mm}"])),
+                        "index_differences": int(diff.size), "of_which_ties": ties}
+    out["test_ascii"] = ta
+    out["all_pass"] = bool(
+        out.get("digest", {}).get("d2_sha256_match", True) and bad == 0
+        and out["fp32_vs_fp64"]["within"]
+        and all(v["d2_bit_identical"] and v["index_differences"] == v["of_which_ties"]
+                for v in ta.values()))
+    return out
+
+
+def c3_sample(ctx, width: int, k: int):
+    """Error of the FP32 and guarded forms against the FP64 form (the reference's
+    arithmetic) on a diagonal sample of the stress series: c3 (n = 8,388,608,
+    m = 1024, 32 planted sine motifs, 16 constant stretches at the walk's level)
+    and c3z (the stretches at level 0), diagonals [m/4 + 1, m/4 + 1 + width).
+    Per form: cells/s on the sample and the error figures of error_report
+    (maximum far from the stretches and near them, windows whose FP64 value is
+    itself inaccurate excluded)."""
+    import thesiscode_b200 as mp
+    from thesiscode_b200 import error_report as er
+    out = {}
+    for name in ("c3", "c3z"):
+        x, m, segs, _ = er.load(name)
+        lo = m // 4 + 1
+        hi = lo + width
+        cells = mp.cells(x.size, m, lo, hi)
+        p64 = ctx.selfjoin(x, m, precision=mp.FP64, diag_lo=lo, diag_hi=hi)
+        j64 = ctx.last_phase_ms()[1]
+        rec = {"diagonals": [lo, hi], "cells": cells, "reanchor_k": k,
+               "fp64_cells_per_s": cells / (j64 * 1e-3)}
+        for form, prec in (("fp32", mp.FP32_REANCHOR), ("guarded", mp.FP32_GUARDED)):
+            p = ctx.selfjoin(x, m, precision=prec, reanchor_k=k, diag_lo=lo, diag_hi=hi)
+            j = ctx.last_phase_ms()[1]
+            r = er.compare(x, m, segs, p64, p, name == "c3z", K=k)
+            rec[form] = {"cells_per_s": cells / (j * 1e-3),
+                         "max_rel_far_from_stretches": r["max_rel_far_from_stretches"],
+                         "max_rel_near_stretches": r["max_rel_near_stretches"],
+                         "mean_rel": r["mean_rel"], "reference_inaccurate": r["reference_inaccurate"]}
+        out[name] = rec
+    return out
+
+
 def run_reference_arm(args, world):
     import thesiscode_b200.workloads as wl
     rank = int(os.environ.get("RANK", "0"))
@@ -169,13 +293,20 @@ def run_reference_arm(args, world):
     cells = sum(c for c, _ in vals)
     sec = sum(s for _, s in vals)
     v = cells / sec
+    import thesiscode_b200 as mp
+    total = mp.cells(x.size, m)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "cells/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * sec / len(vals), "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "c2: random walk n=1,048,576 seed 1, m=256, excl=64; each step a "
-                               "bounded diagonal sample", "n": int(x.size), "m": m},
+                               "bounded diagonal sample (the longest diagonals) timed as a rate",
+                   "n": int(x.size), "m": m, "cells_per_step": cells / len(vals),
+                   "sample_fraction": cells / len(vals) / total,
+                   "cpu_model": cpu_model(), "threads": threads,
+                   "parallelism": "the reference's kernels.cpp (fast-math build) on host threads, "
+                                  "scrimp_triv_par partitioning re-hosted on threads (no MPI)"},
         "cpu_baseline": {"value": v, "unit": "cells/s", "cores": threads, "kind": kind,
                          "sample": sample},
         "e2e": {"value": v, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -280,6 +411,7 @@ def run_ours(args, world):
         tot64 = float(t.item())
     value64 = cells_total * fsteps / (tot64 * 1e-3)
     fp64_d2 = d2.cpu().numpy().copy()
+    fp64_idx = ix.cpu().numpy().copy()
 
     # -- end to end with pinned host buffers ----------------------------------------
     # N = 1: one mp_selfjoin call on host pointers (it copies in and out itself).
@@ -335,6 +467,25 @@ def run_ours(args, world):
         t = torch.tensor([tot_e2e], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         tot_e2e = float(t.item())
+    # the FP64 form end to end: one mp_selfjoin call on pinned host buffers per step
+    e2e64 = None
+    if world == 1:
+        ctx.selfjoin(xh, m, precision=mp.FP64, out=oh, stream=stream.cuda_stream)
+        lat64 = []
+        for _ in range(fsteps):
+            with torch.cuda.stream(stream):
+                flush.fill_(3.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.selfjoin(xh, m, precision=mp.FP64, out=oh, stream=stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            lat64.append(e0.elapsed_time(e1))
+        e2e64 = {"value": cells_total * len(lat64) / (sum(lat64) * 1e-3), "unit": "cells/s",
+                 "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 16 * PL,
+                 "path": "mp_selfjoin (C ABI), FP64 form, pinned host input/outputs"}
+
     e2e = {"value": cells_total * len(lat) / (tot_e2e * 1e-3), "unit": "cells/s",
            "h2d_bytes_per_step": 8 * n * world, "d2h_bytes_per_step": 16 * PL,
            "path": "mp_selfjoin (C ABI) with pinned host input/outputs" if world == 1 else
@@ -359,7 +510,7 @@ def run_ours(args, world):
     dt = np.sqrt(np.abs(fp64_d2))
     rel = np.abs(np.sqrt(np.abs(fp32_d2)) - dt) / dt
     err = {"max_rel": float(rel.max()), "mean_rel": float(rel.mean()),
-           "index_agreement": float(np.mean(fp32_idx == ix.cpu().numpy()))}
+           "index_agreement": float(np.mean(fp32_idx == fp64_idx))}
 
     # roofline of the dominant kernel (the FP32 tile join)
     join_avg_ms = float(np.mean(join_ms)) if join_ms else float("nan")
@@ -403,7 +554,7 @@ def run_ours(args, world):
         "fp64_baseline": {"value": value64, "unit": "cells/s", "ms_per_step": tot64 / fsteps,
                           "kernel": "fp64_band_kernel (reference arithmetic, bit-identical)",
                           "roofline_frac_f64": roof64 / peaks["f64_dfma"] if peaks["f64_dfma"]
-                          else None, "kernel_ms": join64, "phases": phases64},
+                          else None, "kernel_ms": join64, "phases": phases64, "e2e": e2e64},
         # the reference logs "(PL - excl)^2 / t" as its throughput (ScrimpVertBlocked
         # PERF_LOG); the same figure for this run, beside the true cell count
         "reference_log_metric": {"value": float(PL - excl) ** 2 / (total_ms / args.steps * 1e-3),
@@ -417,11 +568,29 @@ def run_ours(args, world):
         "clocks": clocks,
     }
     line["e2e"] = e2e
+    if world == 1 and not args.no_extras:
+        # the batched (c4), serving (c5) and stress-series (c3) forms, summarised
+        ctx.close()
+        ctx = None
+        torch.cuda.empty_cache()
+        b = batch_measure(args.c4_count, 1, 1, 1)
+        line["batch"] = {k: b[k] for k in ("value", "unit", "ms_per_step", "e2e", "config",
+                                           "gpu_launches", "clocks")}
+        srv = serving_measure(args.extra_rates, args.extra_serve_seconds, args.slots, 1)
+        line["serving"] = [{k: r[k] for k in ("rate_hz", "duration_s", "requests", "completed",
+                                              "rejected", "p50_ms", "p99_ms", "queue_p50_ms",
+                                              "cells_per_s", "slots")} for r in srv]
+        with mp.Context(local) as cctx:
+            cctx.set_phase_timing(True)
+            line["c3_sample"] = c3_sample(cctx, args.c3_width, args.reanchor_k)
+        ctx = mp.Context(local)
     if world == 1 and not args.no_cpu_baseline:
+        # the reference's CPU code: parity of this run's profiles, then its speed
+        line["parity"] = parity_checks(ctx, args.workload, x, m, fp64_d2, fp64_idx, fp32_d2)
         threads = host_cores()
         cells, sec, kind, sample = cpu_reference_run(x, m, args.ref_seconds, threads)
         line["cpu_baseline"] = {"value": cells / sec, "unit": "cells/s", "cores": threads,
-                                "kind": kind, "sample": sample}
+                                "kind": kind, "sample": sample, "cpu_model": cpu_model()}
         c1, s1, k1, smp1 = cpu_reference_run(x, m, min(3.0, args.ref_seconds), 1)
         line["cpu_baseline_1core"] = {"value": c1 / s1, "unit": "cells/s", "cores": 1, "kind": k1,
                                       "sample": smp1}
@@ -429,13 +598,13 @@ def run_ours(args, world):
     ctx.close()
 
 
-def run_batch_workload(args):
-    """Workload c4: 4,096 FP32-input walks (lengths log-uniform in [2048,
-    262144], m in {64, 128, 256}) solved by one persistent, graph-captured
-    launch per step; tile widths from the autotuner table.  With --gpus N the
-    series are split into N groups of nearly equal cells (shard.balance_by_cost)
-    and each GPU runs its group as its own batch (replicas, nothing exchanged);
-    a step lasts until the slowest GPU is done."""
+def batch_measure(c4_count, gpus, steps, warmup):
+    """Workload c4: FP32-input walks (lengths log-uniform in [2048, 262144], m in
+    {64, 128, 256}, seed 3) solved by one persistent, graph-captured launch per
+    step; tile widths from the autotuner table.  With gpus > 1 the series are
+    split into groups of nearly equal cells (shard.balance_by_cost) and each GPU
+    runs its group as its own batch (replicas, nothing exchanged); a step lasts
+    until the slowest GPU is done.  Returns the measurement as a dict."""
     import threading
 
     import torch
@@ -443,10 +612,10 @@ def run_batch_workload(args):
     import thesiscode_b200 as mp
     import thesiscode_b200.workloads as wl
     from thesiscode_b200 import shard
-    data = wl.c4(args.c4_count)
+    data = wl.c4(c4_count)
     lens = [x.size for x, _ in data]
     ms = [m for _, m in data]
-    groups = shard.balance_by_cost([mp.cells(n, m) for n, m in zip(lens, ms)], max(1, args.gpus))
+    groups = shard.balance_by_cost([mp.cells(n, m) for n, m in zip(lens, ms)], max(1, gpus))
     reps = []  # (context, batch, stream, series) per GPU with work
     for d, g in enumerate(groups):
         if not g:
@@ -457,14 +626,14 @@ def run_batch_workload(args):
         series = [data[i][0] for i in g]
         b.upload(series, st.cuda_stream)
         reps.append((ctx, b, st, series))
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         for _, b, st, _ in reps:
             b.launch(st.cuda_stream)
     for _, _, st, _ in reps:
         st.synchronize()
     steps_ms = []
     with ClockSampler([d for d, g in enumerate(groups) if g]) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             evs = []
             for _, b, st, _ in reps:
                 e0 = torch.cuda.Event(enable_timing=True)
@@ -491,41 +660,51 @@ def run_batch_workload(args):
         for t in ths:
             t.join()
 
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         run_all()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         run_all()
-    e2e_s = (time.perf_counter() - t0) / args.steps
+    e2e_s = (time.perf_counter() - t0) / steps
     launches = sum(b.launch_count for _, b, _, _ in reps)
-    line = {"metric": "batched self-join cells/s (c4, one persistent graph-captured launch)",
-            "value": cells / (ms_step * 1e-3), "unit": "cells/s", "n_gpus": len(reps),
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "dtype": "f32",
-            "data": "synthetic", "scaling": "strong",
-            "config": {"workload": f"c4: {len(data)} FP32 random walks, lengths log-uniform "
-                                   f"[2048, 262144], m in {{64,128,256}}, seed 3",
-                       "series": len(data), "samples": int(sum(lens)), "cells": cells,
-                       "tiles": sum(b.tiles for _, b, _, _ in reps),
-                       "launches_per_step": launches,
-                       "parallelism": f"{len(reps)} replicas, series balanced by cells"},
-            "e2e": {"value": cells / e2e_s, "unit": "cells/s",
-                    "h2d_bytes_per_step": 4 * int(sum(lens)),
-                    "d2h_bytes_per_step": 16 * int(sum(l - m + 1 for l, m in zip(lens, ms)))},
-            "gpu_launches": launches * args.steps, "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
+    out = {"value": cells / (ms_step * 1e-3), "unit": "cells/s", "n_gpus": len(reps),
+           "steps": steps, "warmup": warmup, "ms_per_step": ms_step, "dtype": "f32",
+           "config": {"workload": f"c4: {len(data)} FP32 random walks, lengths log-uniform "
+                                  f"[2048, 262144], m in {{64,128,256}}, seed 3",
+                      "series": len(data), "samples": int(sum(lens)), "cells": cells,
+                      "tiles": sum(b.tiles for _, b, _, _ in reps),
+                      "launches_per_step": launches,
+                      "parallelism": f"{len(reps)} replicas, series balanced by cells"},
+           "e2e": {"value": cells / e2e_s, "unit": "cells/s",
+                   "h2d_bytes_per_step": 4 * int(sum(lens)),
+                   "d2h_bytes_per_step": 16 * int(sum(l - m + 1 for l, m in zip(lens, ms)))},
+           "gpu_launches": launches * steps, "clocks": clk.summary()}
     for ctx, b, _, _ in reps:
         b.close()
         ctx.close()
+    return out
+
+
+def run_batch_workload(args):
+    line = batch_measure(args.c4_count, args.gpus, args.steps, args.warmup)
+    line = {"metric": "batched self-join cells/s (c4, one persistent graph-captured launch)",
+            **line, "data": "synthetic", "scaling": "strong"}
+    print(json.dumps(line), flush=True)
+
+
+def serving_measure(rates, seconds, slots, gpus):
+    """Workload c5: Poisson request streams at several rates against the
+    continuous-batching server; p50/p99 latency and admitted cells/s per rate."""
+    from thesiscode_b200.serve import run_stream
+    out = []
+    for rate in rates:
+        # gpus > 1: one server per GPU, requests handed out in turn
+        out.append(run_stream(rate, seconds, slots=slots, devices=list(range(max(1, gpus)))))
+    return out
 
 
 def run_serving_workload(args):
-    """Workload c5: Poisson request streams at several rates against the
-    continuous-batching server; p50/p99 latency and admitted cells/s."""
-    from thesiscode_b200.serve import run_stream
-    for rate in args.rates:
-        # --gpus N: one server per GPU, requests handed out in turn
-        r = run_stream(rate, args.serve_seconds, slots=args.slots,
-                       devices=list(range(max(1, args.gpus))))
+    for r in serving_measure(args.rates, args.serve_seconds, args.slots, args.gpus):
         r["metric"] = "serving p50/p99 solve latency (c5)"
         r["n_gpus"] = max(1, args.gpus)
         print(json.dumps(r), flush=True)
@@ -543,6 +722,12 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--slots", type=int, default=32,
                     help="requests the server keeps admitted at once (c5)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default line: skip the c4 batch, c5 serving and c3 accuracy summaries")
+    ap.add_argument("--extra-rates", type=float, nargs="+", default=[10, 30, 100])
+    ap.add_argument("--extra-serve-seconds", type=float, default=6.0)
+    ap.add_argument("--c3-width", type=int, default=32768,
+                    help="diagonals of the c3/c3z accuracy sample in the default line")
     ap.add_argument("--reanchor-k", type=int, default=1024)
     ap.add_argument("--fp64-steps", type=int, default=3)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
