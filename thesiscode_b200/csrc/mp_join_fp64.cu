@@ -58,14 +58,60 @@ __device__ __forceinline__ double4 ld_rec(const double4* p) {
     return make_double4(lo.x, lo.y, hi.x, hi.y);
 }
 
-__device__ __forceinline__ double u2d(unsigned lo, unsigned hi) {
-    return __hiloint2double((int)hi, (int)lo);
-}
-// A 32-byte record of the warp's shared-memory ring.
+// A 32-byte record of the warp's shared-memory ring (16-byte aligned halves).
 __device__ __forceinline__ double4 ring_rec(const char* p) {
-    const uint4 a = lds128(p);
-    const uint4 b = lds128(p + 16);
-    return make_double4(u2d(a.x, a.y), u2d(a.z, a.w), u2d(b.x, b.y), u2d(b.z, b.w));
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    const double2 b = *reinterpret_cast<const double2*>(p + 16);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// Which parts of a column step need the selection, voted over the warp: bit 0
+// when some lane has a cell above its row partial, bit 1 when some cell is
+// above the column's threshold.  One chain of predicated compares per lane
+// (setp ... .or) and two votes; NaN compares false, so NaN cells never select.
+template <int R>
+__device__ __forceinline__ unsigned step_hits(const double (&sc)[R], const double (&acc)[2 * R - 1],
+                                              int b, double tc) {
+    bool row = false, col = false;
+#pragma unroll
+    for (int a = 0; a < R; ++a) {
+        row |= sc[a] > acc[b + a];
+        col |= sc[a] > tc;
+    }
+    return (__any_sync(kFullMask, row) ? 1u : 0u) | (__any_sync(kFullMask, col) ? 2u : 0u);
+}
+template <>
+__device__ __forceinline__ unsigned step_hits<8>(const double (&sc)[8], const double (&acc)[15],
+                                                 int b, double tc) {
+    unsigned r;
+    asm volatile(
+        "{\n\t.reg .pred pr, pc, qr, qc;\n\t"
+        "setp.gt.f64 pr, %1, %9;\n\t"
+        "setp.gt.or.f64 pr, %2, %10, pr;\n\t"
+        "setp.gt.or.f64 pr, %3, %11, pr;\n\t"
+        "setp.gt.or.f64 pr, %4, %12, pr;\n\t"
+        "setp.gt.or.f64 pr, %5, %13, pr;\n\t"
+        "setp.gt.or.f64 pr, %6, %14, pr;\n\t"
+        "setp.gt.or.f64 pr, %7, %15, pr;\n\t"
+        "setp.gt.or.f64 pr, %8, %16, pr;\n\t"
+        "setp.gt.f64 pc, %1, %17;\n\t"
+        "setp.gt.or.f64 pc, %2, %17, pc;\n\t"
+        "setp.gt.or.f64 pc, %3, %17, pc;\n\t"
+        "setp.gt.or.f64 pc, %4, %17, pc;\n\t"
+        "setp.gt.or.f64 pc, %5, %17, pc;\n\t"
+        "setp.gt.or.f64 pc, %6, %17, pc;\n\t"
+        "setp.gt.or.f64 pc, %7, %17, pc;\n\t"
+        "setp.gt.or.f64 pc, %8, %17, pc;\n\t"
+        "vote.sync.any.pred qr, pr, 0xffffffff;\n\t"
+        "vote.sync.any.pred qc, pc, 0xffffffff;\n\t"
+        "selp.u32 %0, 1, 0, qr;\n\t"
+        "@qc or.b32 %0, %0, 2;\n\t"
+        "}"
+        : "=r"(r)
+        : "d"(sc[0]), "d"(sc[1]), "d"(sc[2]), "d"(sc[3]), "d"(sc[4]), "d"(sc[5]), "d"(sc[6]),
+          "d"(sc[7]), "d"(acc[b]), "d"(acc[b + 1]), "d"(acc[b + 2]), "d"(acc[b + 3]),
+          "d"(acc[b + 4]), "d"(acc[b + 5]), "d"(acc[b + 6]), "d"(acc[b + 7]), "d"(tc));
+    return r;
 }
 
 // A threshold as it stands (other warps raise it with atomics meanwhile; any
@@ -104,9 +150,8 @@ __device__ __forceinline__ int thr_off(int t) {
 // score); the lowest winning lane parks (score, row) in the warp's column slot
 // with a predicated store, so no divergent branch splits consecutive steps.
 template <int R>
-__device__ __forceinline__ void select_step(const Fp64BandParams& P, int b, const double (&sc)[R],
-                                            double (&acc_s)[2 * R - 1], int (&acc_a)[2 * R - 1],
-                                            int64_t g0, int lane, double* cslot_s, int* cslot_r) {
+__device__ __forceinline__ void select_rows(int b, const double (&sc)[R], double (&acc_s)[2 * R - 1],
+                                            int (&acc_a)[2 * R - 1]) {
 #pragma unroll
     for (int a = 0; a < R; ++a) {
         if (sc[a] > acc_s[b + a]) {
@@ -114,6 +159,10 @@ __device__ __forceinline__ void select_step(const Fp64BandParams& P, int b, cons
             acc_a[b + a] = a;
         }
     }
+}
+template <int R>
+__device__ __forceinline__ void select_column(const Fp64BandParams& P, int b, const double (&sc)[R],
+                                              int64_t g0, int lane, double* cslot_s, int* cslot_r) {
     // lane's best cell of the column: pairwise tree, left wins ties
     double cb[R];
     int ca[R];
@@ -141,6 +190,13 @@ __device__ __forceinline__ void select_step(const Fp64BandParams& P, int b, cons
         cslot_s[b] = cbest;
         cslot_r[b] = (int)(b + g0 + ca[0]);  // row - jc (rows < 2^31)
     }
+}
+template <int R>
+__device__ __forceinline__ void select_step(const Fp64BandParams& P, int b, const double (&sc)[R],
+                                            double (&acc_s)[2 * R - 1], int (&acc_a)[2 * R - 1],
+                                            int64_t g0, int lane, double* cslot_s, int* cslot_r) {
+    select_rows<R>(b, sc, acc_s, acc_a);
+    select_column<R>(P, b, sc, g0, lane, cslot_s, cslot_r);
 }
 
 // One chunk = R consecutive columns.  FAST chunks hold only cells of the
@@ -171,7 +227,6 @@ __device__ __forceinline__ bool chunk_fp64(const Fp64BandParams& P, int64_t jc, 
         double sc[R];
         if (FAST) {
             const double tc = cthr[b];
-            bool hit = false;
 #pragma unroll
             for (int a = 0; a < R; ++a) {
                 const double4 rv = rwin[(b + a) % R];
@@ -180,11 +235,12 @@ __device__ __forceinline__ bool chunk_fp64(const Fp64BandParams& P, int64_t jc, 
                 const double mm = __dmul_rn(cv.w, rv.w);
                 sc[a] = __fma_rn(qt[a], ss, -mm);
                 qt[a] = __fma_rn(-rv.x, cv.x, __fma_rn(rv.y, cv.y, qt[a]));
-                hit |= (sc[a] > acc_s[b + a]) | (sc[a] > tc);
             }
-            if (__any_sync(kFullMask, hit)) {
+            const unsigned hits = step_hits<R>(sc, acc_s, b, tc);
+            if (hits) {
                 selected = true;
-                select_step<R>(P, b, sc, acc_s, acc_a, g0, lane, cslot_s, cslot_r);
+                if (hits & 1u) select_rows<R>(b, sc, acc_s, acc_a);
+                if (hits & 2u) select_column<R>(P, b, sc, g0, lane, cslot_s, cslot_r);
             }
         } else {
 #pragma unroll
