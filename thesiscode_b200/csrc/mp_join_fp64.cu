@@ -51,13 +51,6 @@ namespace mpgpu {
 
 namespace {
 
-// 32-byte record through the read-only path as two 16-byte loads.
-__device__ __forceinline__ double4 ld_rec(const double4* p) {
-    const double2 lo = __ldg(reinterpret_cast<const double2*>(p));
-    const double2 hi = __ldg(reinterpret_cast<const double2*>(p) + 1);
-    return make_double4(lo.x, lo.y, hi.x, hi.y);
-}
-
 // A 32-byte record of the warp's shared-memory ring (16-byte aligned halves).
 __device__ __forceinline__ double4 ring_rec(const char* p) {
     const double2 a = *reinterpret_cast<const double2*>(p);
@@ -135,12 +128,19 @@ __device__ __forceinline__ void flush_fp64(const Fp64BandParams& P, int shard, i
 }
 
 // Per-warp ring of row thresholds in shared memory, indexed like the record
-// ring (row t of the band at t % kRecRing), one double of padding after every
-// 8 so that lanes reading rows 8 apart hit distinct banks.
-constexpr int kThrRingDoubles = kRecRing + kRecRing / 8;
-__device__ __forceinline__ int thr_off(int t) {
+// ring (row t of the band at slot t % kRecRing), one double of padding after
+// every 8 so that lanes reading rows 8 apart hit distinct banks.  Slots
+// kRecRing .. kRecRing + kThrMirror - 1 mirror slots 0 .. kThrMirror - 1, so
+// the 16 consecutive rows a lane starts in one chunk never wrap: with R = 8
+// their offsets are one base plus compile-time constants.
+constexpr int kThrMirror = 16;
+constexpr int kThrRingDoubles = (kRecRing + kThrMirror) + (kRecRing + kThrMirror) / 8;
+__device__ __forceinline__ int thr_pos(int s) { return s + (s >> 3); }
+__device__ __forceinline__ int thr_off(int t) { return thr_pos(t % kRecRing); }
+__device__ __forceinline__ void thr_store(double* tring, int t, double v) {
     const int s = t % kRecRing;
-    return s + (s >> 3);
+    tring[thr_pos(s)] = v;
+    if (s < kThrMirror) tring[thr_pos(s + kRecRing)] = v;
 }
 
 // The (score, index) selection of one column step: row partials (strict '>',
@@ -211,7 +211,7 @@ __device__ __forceinline__ bool chunk_fp64(const Fp64BandParams& P, int64_t jc, 
                                            const int (&len)[R], const int (&psw)[R],
                                            double (&acc_s)[2 * R - 1], int (&acc_a)[2 * R - 1],
                                            int64_t g0, int lane, double* cslot_s, int* cslot_r,
-                                           const double* cthr) {
+                                           const double* cthr, const char* ccur) {
     bool selected = !FAST;
 #pragma unroll
     for (int b = 0; b < R; ++b) {
@@ -223,7 +223,7 @@ __device__ __forceinline__ bool chunk_fp64(const Fp64BandParams& P, int64_t jc, 
         else
             rwin[(b + R - 1) % R] =
                 ring_rec(rring + rec_off(rec_slot(tbase + b + R - 1)));
-        const double4 cv = ld_rec(P.colrec + j);
+        const double4 cv = ring_rec(ccur + 32 * b);  // column record, staged a chunk ahead
         double sc[R];
         if (FAST) {
             const double tc = cthr[b];
@@ -274,7 +274,7 @@ template <int R>
 __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band, int lane,
                                           int shard, double* ring_s, int* ring_c, char* rring,
                                           double* cslot_s, int* cslot_r, double* tring,
-                                          double* cthr) {
+                                          double* cthr, char* ccol) {
     constexpr int RING = 32 * R;
     const int64_t gb = P.g_lo + band * (int64_t)RING;
     const int64_t g0 = gb + (int64_t)lane * R;
@@ -315,8 +315,13 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
     const double* csrc = P.thr + P.col_key_off;       // threshold of column j
     int fill = 34 * R;
     for (int i = lane; i < 2 * fill; i += 32) rec_store(rring, i >> 1, i & 1, __ldg(rsrc + i));
-    for (int i = lane; i < fill; i += 32) tring[thr_off(i)] = ld_thr(tsrc + i);
+    for (int i = lane; i < fill; i += 32) thr_store(tring, i, ld_thr(tsrc + i));
     if (lane < R) cthr[lane] = ld_thr(csrc + lane);
+    // column records of a chunk in shared memory, double-buffered: R records of
+    // 32 bytes per buffer, the next chunk's loaded while this one runs
+    const uint4* csrc_rec = reinterpret_cast<const uint4*>(P.colrec);
+    if (lane < 2 * R) *reinterpret_cast<uint4*>(ccol + 16 * lane) = __ldg(csrc_rec + lane);
+    int cbuf = 0;
     __syncwarp();
     // register window of row records: slot (k mod R) holds row g0 + jc + k
     double4 rwin[R];
@@ -341,16 +346,19 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
             tnext = ld_thr(tsrc + fill + lane);
             cnext = ld_thr(csrc + jc + R + lane);
         }
+        uint4 cnrec = make_uint4(0, 0, 0, 0);  // next chunk's column records
+        if (lane < 2 * R) cnrec = __ldg(csrc_rec + 2 * (jc + R) + lane);
+        const char* ccur = ccol + cbuf * (32 * R);
         const int tbase = (int)jc + lane * R;
         const char* rbase = rring + rec_off(rec_slot(tbase + R - 1));
         const bool fast = __all_sync(kFullMask, jc + R - 1 <= minpsw);
         bool sel;
         if (fast)
             sel = chunk_fp64<R, true>(P, jc, rring, rbase, tbase, rwin, qt, len, psw, acc_s, acc_a,
-                                      g0, lane, cslot_s, cslot_r, cthr);
+                                      g0, lane, cslot_s, cslot_r, cthr, ccur);
         else
             sel = chunk_fp64<R, false>(P, jc, rring, rbase, tbase, rwin, qt, len, psw, acc_s, acc_a,
-                                       g0, lane, cslot_s, cslot_r, cthr);
+                                       g0, lane, cslot_s, cslot_r, cthr, ccur);
         __syncwarp();
         // the chunk's column maxima (one per column, parked by the winning lane)
         if (sel && lane < R) {
@@ -362,9 +370,11 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
         }
         if (lane < 2 * R) rec_store(rring, fill + (lane >> 1), lane & 1, next);
         if (lane < R) {
-            tring[thr_off(fill + lane)] = tnext;
+            thr_store(tring, fill + lane, tnext);
             cthr[lane] = cnext;
         }
+        if (lane < 2 * R) *reinterpret_cast<uint4*>(ccol + (cbuf ^ 1) * (32 * R) + 16 * lane) = cnrec;
+        cbuf ^= 1;
         fill += R;
         // rows jc + g0 + [0, R) are done for this lane: merge its candidates
         // (selected in this chunk or the previous one) into the ring
@@ -395,10 +405,21 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
             acc_a[k] = acc_a[k + R];
         }
         // new rows jc + R + g0 + k start at their thresholds
+        if (R == 8) {
+            // rows tbase + 8 + k: slot s0 + k with s0 = (tbase + 8) % kRecRing a
+            // multiple of 8 and k < 16 (the mirror keeps them from wrapping)
+            const double* tb = tring + thr_pos((tbase + 8) % kRecRing);
 #pragma unroll
-        for (int k = R - 1; k < 2 * R - 1; ++k) {
-            acc_s[k] = tring[thr_off(tbase + R + k)];
-            acc_a[k] = -1;
+            for (int k = R - 1; k < 2 * R - 1; ++k) {
+                acc_s[k] = tb[k + (k >> 3)];
+                acc_a[k] = -1;
+            }
+        } else {
+#pragma unroll
+            for (int k = R - 1; k < 2 * R - 1; ++k) {
+                acc_s[k] = tring[thr_off(tbase + R + k)];
+                acc_a[k] = -1;
+            }
         }
     }
 
@@ -432,7 +453,7 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
 template <int R>
 constexpr int fp64_smem_bytes() {
     return kFp64WarpsPerBlock *
-           (kRecRingBytes + (32 * R + R) * (int)(sizeof(double) + sizeof(int)) +
+           (kRecRingBytes + 2 * 32 * R + (32 * R + R) * (int)(sizeof(double) + sizeof(int)) +
             (kThrRingDoubles + R) * (int)sizeof(double));
 }
 
@@ -445,6 +466,8 @@ __global__ void __launch_bounds__(32 * kFp64WarpsPerBlock) fp64_band_kernel(cons
     char* p = smem_fp64;
     char* rring = p + w * kRecRingBytes;
     p += kW * kRecRingBytes;
+    char* ccol = p + w * (2 * 32 * R);
+    p += kW * 2 * 32 * R;
     double* tring = reinterpret_cast<double*>(p) + w * kThrRingDoubles;
     p += kW * kThrRingDoubles * sizeof(double);
     double* ring_s = reinterpret_cast<double*>(p) + w * 32 * R;
@@ -466,7 +489,8 @@ __global__ void __launch_bounds__(32 * kFp64WarpsPerBlock) fp64_band_kernel(cons
     for (int64_t r = 0;; ++r) {
         const int64_t band = r * W + ((r & 1) ? W - 1 - wid : wid);
         if (band >= P.nbands) break;
-        band_fp64<R>(P, band, lane, shard, ring_s, ring_c, rring, cslot_s, cslot_r, tring, cthr);
+        band_fp64<R>(P, band, lane, shard, ring_s, ring_c, rring, cslot_s, cslot_r, tring, cthr,
+                     ccol);
     }
 }
 
