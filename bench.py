@@ -265,7 +265,10 @@ def c3_sample(ctx, width: int, k: int):
         p64 = ctx.selfjoin(x, m, precision=mp.FP64, diag_lo=lo, diag_hi=hi)
         j64 = ctx.last_phase_ms()[1]
         rec = {"diagonals": [lo, hi], "cells": cells, "reanchor_k": k,
-               "fp64_cells_per_s": cells / (j64 * 1e-3)}
+               "fp64_cells_per_s": cells / (j64 * 1e-3),
+               "note": "a sample of few long diagonals: the FP64 form's bands (256 diagonals "
+                       "each) fill under one wave of the GPU, so its rate here is not the full "
+                       "join's; the FP32 form's tiles fill it"}
         for form, prec in (("fp32", mp.FP32_REANCHOR), ("guarded", mp.FP32_GUARDED)):
             p = ctx.selfjoin(x, m, precision=prec, reanchor_k=k, diag_lo=lo, diag_hi=hi)
             j = ctx.last_phase_ms()[1]
