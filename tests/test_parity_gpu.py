@@ -256,3 +256,18 @@ def test_selfjoin_ranges_one_call_equals_separate_calls(gpu_ctx, oracle):
         gpu_ctx.selfjoin_ranges(x, m, shard.rank_ranges(x.size, m, 0, 2),
                                 precision=mp.FP32_GUARDED)
     assert e.value.status == mp.MP_ERR_NOT_SUPPORTED
+
+
+def test_fp64_exact_repeats_keep_reference_values_and_tie_rule(gpu_ctx, oracle):
+    """A series made of exact repeats of one pattern (plus a drifting copy), so
+    that many cells share the same score: the threshold-pruned selection must
+    still give the reference's values bit for bit and neighbours that tie with
+    the reference's in its own arithmetic."""
+    rng = np.random.default_rng(77)
+    pattern = np.cumsum(rng.standard_normal(300))
+    x = np.concatenate([pattern, pattern, pattern + 5.0, pattern, pattern * 2.0, pattern])
+    for m in (32, 100):
+        d2, idx = oracle.selfjoin(x, m)
+        p = gpu_ctx.selfjoin(x, m, precision=mp.FP64)
+        assert np.array_equal(p.dist2, d2), m
+        check_fp64_indices(oracle, x, m, p.dist2, p.index, idx)

@@ -20,44 +20,50 @@ namespace mpgpu {
 // ---- reference-exact statistics -------------------------------------------
 
 // cs[i] = A[i] + cs[i-1], cs2[i] = A[i]*A[i] + cs2[i-1] in index order
-// (ScrimpSequOpt.cpp:43-49).  The chain is inherently serial, so one thread
-// runs it -- out of shared memory: the block's other warps load the next chunk
-// of A and write the previous chunk's sums back (both coalesced) while thread 0
-// walks the current one, so the chain never waits for global memory.  Launch
-// with kPrefixThreads threads in one block.
+// (ScrimpSequOpt.cpp:43-49).  Each chain is inherently serial, so lane 0 of
+// warp 0 runs the sum of A and lane 1 the sum of A*A, side by side, out of
+// shared memory: the block's other warps load the next chunk of A and write
+// the previous chunk's sums back (both coalesced) meanwhile, so neither chain
+// waits for global memory.  Launch with kPrefixThreads threads in one block.
 __global__ void __launch_bounds__(kPrefixThreads)
     ref_prefix_kernel(const double* __restrict__ A, int64_t n, double* __restrict__ cs,
                       double* __restrict__ cs2) {
     constexpr int C = kPrefixChunk;
     __shared__ double in[2][C];
-    __shared__ double o1[2][C];
-    __shared__ double o2[2][C];
+    __shared__ double out[2][2][C];  // [chain][buffer][k]: chain 0 sums A, chain 1 sums A*A
     if (blockIdx.x != 0) return;
     const int t = threadIdx.x;
     const int64_t nch = (n + C - 1) / C;
     for (int k = t; k < C; k += blockDim.x) in[0][k] = k < n ? A[k] : 0.0;
     __syncthreads();
-    double s = 0.0, s2 = 0.0;
+    double acc = 0.0;
     for (int64_t c = 0; c < nch; ++c) {
         const int b = (int)(c & 1);
-        if (t == 0) {
+        if (t < 2) {
             const int64_t base = c * C;
             const int cnt = (int)min((int64_t)C, n - base);
+            const double* src = in[b];
+            double* dst = out[t][b];
             int k = 0;
             if (base == 0) {
-                s = in[b][0];
-                s2 = __dmul_rn(s, s);
-                o1[b][0] = s;
-                o2[b][0] = s2;
+                acc = t == 0 ? src[0] : __dmul_rn(src[0], src[0]);
+                dst[0] = acc;
                 k = 1;
             }
-#pragma unroll 8
+            for (; k + 8 <= cnt; k += 8) {
+                double a[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) a[i] = src[k + i];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    acc = __dadd_rn(t == 0 ? a[i] : __dmul_rn(a[i], a[i]), acc);
+                    dst[k + i] = acc;
+                }
+            }
             for (; k < cnt; ++k) {
-                const double a = in[b][k];
-                s = __dadd_rn(a, s);
-                s2 = __dadd_rn(__dmul_rn(a, a), s2);
-                o1[b][k] = s;
-                o2[b][k] = s2;
+                const double a = src[k];
+                acc = __dadd_rn(t == 0 ? a : __dmul_rn(a, a), acc);
+                dst[k] = acc;
             }
         } else if (t >= 32) {
             const int tt = t - 32, nt = blockDim.x - 32;
@@ -69,8 +75,8 @@ __global__ void __launch_bounds__(kPrefixThreads)
             if (c >= 1)
                 for (int k = tt; k < C; k += nt) {
                     const int64_t i = (c - 1) * C + k;
-                    cs[i] = o1[b ^ 1][k];
-                    cs2[i] = o2[b ^ 1][k];
+                    cs[i] = out[0][b ^ 1][k];
+                    cs2[i] = out[1][b ^ 1][k];
                 }
         }
         __syncthreads();
@@ -79,8 +85,8 @@ __global__ void __launch_bounds__(kPrefixThreads)
     for (int k = t; k < C; k += blockDim.x) {
         const int64_t i = c * C + k;
         if (i < n) {
-            cs[i] = o1[c & 1][k];
-            cs2[i] = o2[c & 1][k];
+            cs[i] = out[0][c & 1][k];
+            cs2[i] = out[1][c & 1][k];
         }
     }
 }
