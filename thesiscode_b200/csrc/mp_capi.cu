@@ -111,19 +111,20 @@ int fp64_shards(int64_t PL) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(16, s));
 }
 
-// Diagonals per lane: 8 amortises the per-column warp reduction best; fewer
-// only when the band count would leave SMs idle (>= 4 warps per SM wanted).
+// Diagonals per lane.  Every band walks all of its columns, so the longest
+// band's column count is the critical path whatever R is; R = 8 does the most
+// cells per step and was fastest at every size measured on a B200 (FP64 join,
+// m = 256: n = 16,384 -> 3.2 ms vs 3.6 ms at R = 4 and 5.2 ms at R = 2, even
+// with 63 bands for 148 SMs; n = 524,288 -> 121 vs 190 vs 482 ms).  Only a few
+// hundred diagonals (the kernel API's blocks) leave most lanes of an R = 8
+// band idle; there narrower bands spread the same steps over more warps.
 int pick_fp64_R(int64_t ndiag) {
 #ifdef MPGPU_FP64_FORCE_R
     return MPGPU_FP64_FORCE_R;  // tuning builds only
 #endif
-    const int sms = sm_count();
-    for (int R : {8, 4}) {
-        const int64_t nb = (ndiag + 32 * R - 1) / (32 * R);
-        if ((nb + 1) / 2 >= (int64_t)sms * 4) return R;
-    }
-    const int64_t nb2 = (ndiag + 63) / 64;
-    return (nb2 + 1) / 2 >= sms ? 2 : 1;
+    if (ndiag >= 2048) return 8;
+    if (ndiag >= 512) return 4;
+    return ndiag >= 128 ? 2 : 1;
 }
 
 int launch_band(int R, const Fp64BandParams& P, cudaStream_t s) {

@@ -74,6 +74,30 @@ __device__ __forceinline__ unsigned step_hits(const double (&sc)[R], const doubl
     return (__any_sync(kFullMask, row) ? 1u : 0u) | (__any_sync(kFullMask, col) ? 2u : 0u);
 }
 template <>
+__device__ __forceinline__ unsigned step_hits<4>(const double (&sc)[4], const double (&acc)[7],
+                                                 int b, double tc) {
+    unsigned r;
+    asm volatile(
+        "{\n\t.reg .pred pr, pc, qr, qc;\n\t"
+        "setp.gt.f64 pr, %1, %5;\n\t"
+        "setp.gt.or.f64 pr, %2, %6, pr;\n\t"
+        "setp.gt.or.f64 pr, %3, %7, pr;\n\t"
+        "setp.gt.or.f64 pr, %4, %8, pr;\n\t"
+        "setp.gt.f64 pc, %1, %9;\n\t"
+        "setp.gt.or.f64 pc, %2, %9, pc;\n\t"
+        "setp.gt.or.f64 pc, %3, %9, pc;\n\t"
+        "setp.gt.or.f64 pc, %4, %9, pc;\n\t"
+        "vote.sync.any.pred qr, pr, 0xffffffff;\n\t"
+        "vote.sync.any.pred qc, pc, 0xffffffff;\n\t"
+        "selp.u32 %0, 1, 0, qr;\n\t"
+        "@qc or.b32 %0, %0, 2;\n\t"
+        "}"
+        : "=r"(r)
+        : "d"(sc[0]), "d"(sc[1]), "d"(sc[2]), "d"(sc[3]), "d"(acc[b]), "d"(acc[b + 1]),
+          "d"(acc[b + 2]), "d"(acc[b + 3]), "d"(tc));
+    return r;
+}
+template <>
 __device__ __forceinline__ unsigned step_hits<8>(const double (&sc)[8], const double (&acc)[15],
                                                  int b, double tc) {
     unsigned r;
