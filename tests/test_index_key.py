@@ -1,7 +1,9 @@
 """The FP64 form's index key (idx_key_f64, thesiscode_b200/csrc/mp_common.cuh)
 on CPU.  Profiles are max-merged on this 64-bit key, so it must order
 candidates by v = m - score (half the squared distance; smaller v wins), break
-equal high parts toward the smaller neighbour, put v <= 0 above every v > 0,
+equal high parts toward the smaller neighbour, put v <= 0 above every v > 0
+(and order v <= 0 by |v| up to inf, for the huge scores of near-constant
+windows),
 keep ~33 mantissa bits at idx_bits = 24 (ties only within ~1.2e-10 relative),
 and give back the neighbour from its low bits.  Compiled with nvcc as a host
 program (the key function is host-callable)."""
@@ -17,6 +19,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, "thesiscode_b200", "csrc")
 
 PROGRAM = r"""
+#include <cfloat>
+#include <cmath>
 #include <cstdio>
 #include <random>
 #include "mp_common.cuh"
@@ -88,6 +92,36 @@ int main() {
                 const unsigned long long kb_ = idx_key_f64(m - below, (double)m, 0, idx_bits, vlo);
                 const unsigned long long ka_ = idx_key_f64(m - at, (double)m, 0, idx_bits, vlo);
                 if (m - (m - below) < m - (m - at)) CHECK(kb_ >= ka_, "binade e=%d", e);
+            }
+            // v <= 0 (score >= m, e.g. the huge scores of a window whose variance
+            // rounds to a tiny positive value): the key grows with |v| over the
+            // whole double range -- through the end of the fine region at
+            // 2^(t-32) and up to inf -- strictly once |v| > vlo, and stays above
+            // every v > 0.  score = |v| with m = 0 keeps v exact.
+            {
+                const unsigned long long top_pos =
+                    idx_key_f64(-std::ldexp(1.0, t - 64), 0.0, 0, idx_bits, vlo) >> idx_bits;
+                unsigned long long prev = idx_key_f64(0.0, 0.0, 0, idx_bits, vlo) >> idx_bits;
+                CHECK(prev > top_pos, "region at v = 0");
+                for (int e = t - 70; e < 1023; ++e) {
+                    for (double f : {1.0, 1.3, 1.7}) {
+                        const double a = std::ldexp(f, e);
+                        const unsigned long long k = idx_key_f64(a, 0.0, 0, idx_bits, vlo) >> idx_bits;
+                        if (a > std::ldexp(1.0, t - 64)) CHECK(k > prev, "neg order |v|=%.17g", a);
+                        else CHECK(k == prev, "neg clamp |v|=%.17g", a);
+                        prev = k;
+                    }
+                }
+                const double edge = std::ldexp(1.0, t - 32);
+                const unsigned long long kin =
+                    idx_key_f64(std::nextafter(edge, 0.0), 0.0, 0, idx_bits, vlo) >> idx_bits;
+                const unsigned long long kout = idx_key_f64(edge, 0.0, 0, idx_bits, vlo) >> idx_bits;
+                CHECK(kout > kin, "fine/coarse edge");
+                const unsigned long long kinf =
+                    idx_key_f64(HUGE_VAL, 0.0, 0, idx_bits, vlo) >> idx_bits;
+                const unsigned long long kmax = idx_key_f64(DBL_MAX, 0.0, 0, idx_bits, vlo) >> idx_bits;
+                CHECK(kinf >= kmax && kmax >= prev, "top of the range");
+                CHECK(kinf < (1ull << (64 - idx_bits)), "field overflow");
             }
         }
     }

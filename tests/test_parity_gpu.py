@@ -106,6 +106,31 @@ def test_fp64_diagonal_range(gpu_ctx, oracle):
         check_fp64_indices(oracle, x, m, p.dist2, p.index, idx)
 
 
+def flat_dense_series(n=16000, m=32, every=200, seed=12):
+    """Random walk with a constant segment of 2m samples (held at the walk's
+    value, so the windows' variance rounds to 0 or below and sInv is inf or
+    NaN) every `every` samples."""
+    x = workloads.random_walk(n, seed)
+    for s in range(50, n - 2 * m, every):
+        x[s:s + 2 * m] = x[s]
+    return x, m
+
+
+@pytest.mark.parametrize("width", [100, 300, 1000, 3000])
+def test_fp64_nan_cells_beside_valid_cells(gpu_ctx, oracle, width):
+    """NaN cells of constant windows never select, and never hide the valid
+    cell beside them in a lane's R diagonals (band widths 100..3000 give
+    R = 1, 2, 4, 8), in full bands and in a range's partial last band."""
+    x, m = flat_dense_series()
+    PL = x.size - m + 1
+    for lo in (m // 4 + 1, PL // 3, PL - width):
+        hi = min(lo + width, PL)
+        d2, idx = oracle.selfjoin(x, m, diag_lo=lo, diag_hi=hi)
+        p = gpu_ctx.selfjoin(x, m, precision=mp.FP64, diag_lo=lo, diag_hi=hi)
+        assert np.array_equal(p.dist2, d2, equal_nan=True), (width, lo, hi)
+        check_fp64_indices(oracle, x, m, p.dist2, p.index, idx)
+
+
 def test_fp64_device_pointers_match_host(gpu_ctx):
     import torch
     x = workloads.random_walk(30000, 4)

@@ -124,20 +124,33 @@ __host__ __device__ __forceinline__ long long f64_bits(double v) {
 // vlo = 2^(t-64), where the host picks t with 2^t > 2m + 2, so that 64
 // binades need 6 exponent bits instead of 11 and the freed bits keep mantissa
 // (33 mantissa bits at idx_bits = 24: candidates closer than ~1.2e-10 in
-// relative squared distance share a high part).  |v| outside [vlo, 2^t)
-// clamps to the range ends.
+// relative squared distance share a high part).  For v > 0, |v| outside
+// [vlo, 2^t) clamps to the range ends (no candidate above the floor score -1
+// has v >= 2^t).  For v <= 0 (score >= m) the first 32 binades [vlo, 2^(t-32))
+// keep that resolution -- scores a rounding error above m land there -- and
+// every larger |v| up to inf (scores far above m, from the huge sInv of a
+// window whose variance rounds to a tiny positive value) goes to a coarser
+// region above them: all 11 exponent bits and 51 - idx_bits mantissa bits, so
+// the key stays monotone in the score over the whole double range.
 __host__ __device__ __forceinline__ unsigned long long idx_key_f64(double score, double m,
                                                                    unsigned long long neighbour,
                                                                    int idx_bits, long long vlo_bits) {
     const unsigned long long lowmask = (1ull << idx_bits) - 1ull;
     const int shift = idx_bits > 5 ? idx_bits - 5 : 0;
     const long long span = 1ll << 58;  // 64 binades of 2^52 bit patterns
+    const long long fine = 1ll << 57;  // 32 binades
     const double v = m - score;
     long long x = f64_bits(fabs(v)) - vlo_bits;
-    x = x < 0 ? 0 : (x > span - 1 ? span - 1 : x);
-    const unsigned long long field =
-        v > 0.0 ? (unsigned long long)(span - 1 - x) >> shift
-                : (1ull << (63 - idx_bits)) | ((unsigned long long)x >> shift);
+    x = x < 0 ? 0 : x;
+    unsigned long long field;
+    if (v > 0.0) {
+        field = (unsigned long long)(span - 1 - (x > span - 1 ? span - 1 : x)) >> shift;
+    } else {
+        const unsigned long long low =
+            x < fine ? (unsigned long long)x >> shift
+                     : (1ull << (62 - idx_bits)) | ((unsigned long long)(x - fine) >> (idx_bits + 1));
+        field = (1ull << (63 - idx_bits)) | low;
+    }
     return (field << idx_bits) | (lowmask - neighbour);
 }
 

@@ -187,12 +187,14 @@ __device__ __forceinline__ void select_rows(int b, const double (&sc)[R], double
 template <int R>
 __device__ __forceinline__ void select_column(const Fp64BandParams& P, int b, const double (&sc)[R],
                                               int64_t g0, int lane, double* cslot_s, int* cslot_r) {
-    // lane's best cell of the column: pairwise tree, left wins ties
+    // lane's best cell of the column: pairwise tree, left wins ties.  A NaN
+    // cell (a constant window) never selects under the reference's '>'; as
+    // -DBL_MAX it also cannot hide the cell it is paired with in the tree.
     double cb[R];
     int ca[R];
 #pragma unroll
     for (int a = 0; a < R; ++a) {
-        cb[a] = sc[a];
+        cb[a] = sc[a] == sc[a] ? sc[a] : -DBL_MAX;
         ca[a] = a;
     }
 #pragma unroll
