@@ -55,6 +55,12 @@ static_assert(sizeof(RowRec) == 32, "row record is 32 bytes");
 constexpr unsigned kTagMask = 0xffu;
 constexpr float kInf = __builtin_huge_valf();
 
+// Terms of the FP64 anchor staged per pass: the column's chunk plus the warp's
+// 32*8 + chunk rows (skewed by 1/8) must fit the record ring.
+constexpr int kAnchorChunk = 512;
+static_assert(8 * (kAnchorChunk + (32 * 8 + kAnchorChunk) * 9 / 8) <= kRecRingBytes,
+              "anchor staging fits the record ring");
+
 __device__ __forceinline__ float tag_key(float u, unsigned tag) {
     return __uint_as_float((__float_as_uint(u) & ~kTagMask) | tag);
 }
@@ -203,37 +209,65 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
     for (int a = 0; a < R; ++a) tag[a] = ((unsigned)lane << 3) | (unsigned)a;
 
     // ---- FP64 re-anchor: cov(j0, j0+g) for the lane's R diagonals ----------
+    // The series terms are staged in the (not yet used) record ring with
+    // coalesced loads, kAnchorChunk terms at a time: the column's A[j0 + k]
+    // and the warp's rows A[j0 + gb + i], i < 32R + chunk, skewed by one double
+    // per 8 so that lanes reading rows 8 apart hit distinct banks.  Each lane
+    // then sums its R products in k order from shared memory.
+    double mu0 = (double)P.m * __ldg(P.mean + j0);
+    double mr[R];
+#pragma unroll
+    for (int a = 0; a < R; ++a) mr[a] = __ldg(P.mean + j0 + g0 + a);
     double q[R];
 #pragma unroll
     for (int a = 0; a < R; ++a) q[a] = 0.0;
     {
+        static_assert(R % 8 == 0, "anchor row skew assumes lanes start on multiples of 8 rows");
+        double* scol = reinterpret_cast<double*>(rring);
+        double* srow = scol + kAnchorChunk;
         const double* Ac = P.A + j0;
-        const double* Aw = P.A + j0 + g0;
-        double w[R];
+        const double* Ar = P.A + j0 + gb;
+        // lane's rows i = lane*R + t sit at srow[lane*(R + R/8) + t + t/8]
+        const double* wl = srow + lane * (R + R / 8);
+        for (int64_t kb0 = 0; kb0 < P.m; kb0 += kAnchorChunk) {
+            const int kc = (int)min((int64_t)kAnchorChunk, P.m - kb0);
+            __syncwarp();
+#pragma unroll 4
+            for (int i = lane; i < kc; i += 32) scol[i] = __ldg(Ac + kb0 + i);
+#pragma unroll 4
+            for (int i = lane; i < 32 * R + kc; i += 32) srow[i + (i >> 3)] = __ldg(Ar + kb0 + i);
+            __syncwarp();
+            double w[R];
 #pragma unroll
-        for (int a = 0; a < R - 1; ++a) w[a] = __ldg(Aw + a);
-        int64_t k0 = 0;
-        for (; k0 + R <= P.m; k0 += R) {
+            for (int a = 0; a < R - 1; ++a) w[a] = wl[a];
+            int k = 0;
+            for (; k + R <= kc; k += R) {
+                const double* wk = wl + (k / 8) * 9;  // row lane*R + k, k % 8 == 0
 #pragma unroll
-            for (int kk = 0; kk < R; ++kk) {
-                w[(kk + R - 1) % R] = __ldg(Aw + k0 + kk + R - 1);
-                const double x = __ldg(Ac + k0 + kk);
+                for (int kk = 0; kk < R; ++kk) {
+                    const int t = kk + R - 1;
+                    w[(kk + R - 1) % R] = wk[t + (t >> 3)];
+                    const double x = scol[k + kk];
 #pragma unroll
-                for (int a = 0; a < R; ++a) q[a] = __fma_rn(x, w[(kk + a) % R], q[a]);
+                    for (int a = 0; a < R; ++a) q[a] = __fma_rn(x, w[(kk + a) % R], q[a]);
+                }
+            }
+            for (; k < kc; ++k) {
+                const double x = scol[k];
+#pragma unroll
+                for (int a = 0; a < R; ++a) {
+                    const int t = k + a;
+                    q[a] = __fma_rn(x, wl[t + (t >> 3)], q[a]);
+                }
             }
         }
-        for (int64_t k = k0; k < P.m; ++k) {
-            const double x = __ldg(Ac + k);
-#pragma unroll
-            for (int a = 0; a < R; ++a) q[a] = __fma_rn(x, __ldg(Aw + k + a), q[a]);
-        }
+        __syncwarp();
     }
     float2 nc2[H];
     {
-        const double mu0 = (double)P.m * __ldg(P.mean + j0);
         float nc[R];
 #pragma unroll
-        for (int a = 0; a < R; ++a) nc[a] = (float)__fma_rn(mu0, __ldg(P.mean + j0 + g0 + a), -q[a]);
+        for (int a = 0; a < R; ++a) nc[a] = (float)__fma_rn(mu0, mr[a], -q[a]);
 #pragma unroll
         for (int a = 0; a < H; ++a) nc2[a] = make_float2(nc[a], nc[a + H]);
     }
