@@ -55,6 +55,12 @@ static_assert(sizeof(RowRec) == 32, "row record is 32 bytes");
 constexpr unsigned kTagMask = 0xffu;
 constexpr float kInf = __builtin_huge_valf();
 
+// Row-partial ring: 34 chunks of 8 rows, 12 floats apart (48 bytes), so that
+// the 8 lanes of a quarter-warp merging their chunks with 16-byte accesses
+// hit 8 distinct groups of 4 banks (a 32-byte stride would pair them up).
+constexpr int kRowChunks = 34;
+constexpr int kRowStride = 12;
+
 // Terms of the FP64 anchor staged per pass: the column's chunk plus the warp's
 // 32*8 + chunk rows (skewed by 1/8) must fit the record ring.
 constexpr int kAnchorChunk = 512;
@@ -273,7 +279,7 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
     }
 
     // ---- ring of row partials for this tile -----------------------------------
-    for (int k = lane; k < 34 * R; k += 32) ring[k] = kInf;
+    for (int k = lane; k < kRowChunks * kRowStride; k += 32) ring[k] = kInf;
     __syncwarp();
 
     // row partials: row o of chunk c (o in [0, 2R-1)) lives in acc[(o + R*(c%2)) % 2R]
@@ -300,11 +306,13 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
         win[k].nn = *reinterpret_cast<const float2*>(p + 16);
     }
 
-    // Row partials leave the registers through a ring of RK slots in shared
-    // memory: row t of the tile sits at ((t / R) % RK_CHUNKS) * R + t % R.
-    // With RK_CHUNKS = 34 the rows finished by lane 0 in a chunk pair stay put
-    // until they are flushed at the end of the pair.
-    constexpr int RK_CHUNKS = 34;
+    // Row partials leave the registers through a ring of kRowChunks chunks of
+    // R rows in shared memory: row t of the tile sits at
+    // ((t / R) % kRowChunks) * kRowStride + t % R.  With 34 chunks the rows
+    // finished by lane 0 in a chunk pair stay put until they are flushed at the
+    // end of the pair.
+    constexpr int RK_CHUNKS = kRowChunks;
+    static_assert(R == 8, "row ring stride is laid out for 8 rows per chunk");
     int cb = 0;                              // column buffer of the current pair
     int rslot = rec_slot(lane * R + H - 1);  // record slot of jr + lane*R + H - 1
     int kslot = lane;                        // (jr / R + lane) % RK_CHUNKS
@@ -337,7 +345,7 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
             }
             // this chunk's lower half (rows jh + g0 + [0, R)) is final for the lane
             const int ks = (kslot + half) >= RK_CHUNKS ? kslot + half - RK_CHUNKS : kslot + half;
-            float4* rv4 = reinterpret_cast<float4*>(ring + ks * R);
+            float4* rv4 = reinterpret_cast<float4*>(ring + ks * kRowStride);
 #pragma unroll
             for (int v = 0; v < R / 4; ++v) {
                 float4 t = rv4[v];
@@ -347,6 +355,8 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
                 t.w = fminf(t.w, acc[(4 * v + 3 + half * R) % (2 * R)]);
                 rv4[v] = t;
             }
+            // lane l's next merge reads the chunk lane l + 1 has just written
+            __syncwarp();
         }
         kslot += 2;
         if (kslot >= RK_CHUNKS) kslot -= RK_CHUNKS;
@@ -363,7 +373,7 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
             }
             // rows jr + [0, 2R) of the tile have met every lane: flush, free
             const int c = jr / R + (lane >> 3);
-            const int e = (c % RK_CHUNKS) * R + (lane & (R - 1));
+            const int e = (c % RK_CHUNKS) * kRowStride + (lane & (R - 1));
             const float v = ring[e];
             ring[e] = kInf;
             flush_row<R>(P, v, j0 + gb + jr + lane, gb, ulim);
@@ -377,7 +387,7 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
 
     // drain: the carried upper half (rows jr + lane*R + [0, R-1)), then every slot
     {
-        float* base = ring + kslot * R;
+        float* base = ring + kslot * kRowStride;
 #pragma unroll
         for (int k = 0; k < R - 1; ++k) base[k] = fminf(base[k], acc[k]);
     }
@@ -386,14 +396,15 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
     for (int e = lane; e < RK_CHUNKS * R; e += 32) {
         const int cs = e / R;
         const int rel = (cs - cend % RK_CHUNKS + RK_CHUNKS) % RK_CHUNKS;
-        flush_row<R>(P, ring[e], j0 + gb + (int64_t)(cend + rel) * R + (e % R), gb, ulim);
+        flush_row<R>(P, ring[cs * kRowStride + e % R], j0 + gb + (int64_t)(cend + rel) * R + (e % R),
+                     gb, ulim);
     }
     __syncwarp();
 }
 
 constexpr int kFp32WarpsPerBlock = 4;
 
-constexpr int kRowKeySlots = 34 * 8;
+constexpr int kRowKeySlots = kRowChunks * kRowStride;
 template <int R>
 constexpr int fp32_smem_bytes() {
     return kFp32WarpsPerBlock * (kRecRingBytes + kRowKeySlots * (int)sizeof(float) + 4 * 32 * R);
