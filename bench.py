@@ -264,16 +264,18 @@ def c3_sample(ctx, width: int, k: int):
         cells = mp.cells(x.size, m, lo, hi)
         p64 = ctx.selfjoin(x, m, precision=mp.FP64, diag_lo=lo, diag_hi=hi)
         j64 = ctx.last_phase_ms()[1]
-        rec = {"diagonals": [lo, hi], "cells": cells, "reanchor_k": k,
+        rec = {"diagonals": [lo, hi], "cells": cells,
                "fp64_cells_per_s": cells / (j64 * 1e-3),
                "note": "a sample of few long diagonals: the FP64 form's bands (256 diagonals "
                        "each) fill under one wave of the GPU, so its rate here is not the full "
                        "join's; the FP32 form's tiles fill it"}
-        for form, prec in (("fp32", mp.FP32_REANCHOR), ("guarded", mp.FP32_GUARDED)):
-            p = ctx.selfjoin(x, m, precision=prec, reanchor_k=k, diag_lo=lo, diag_hi=hi)
+        # each form at its re-anchor interval: k for the FP32 form, the guarded
+        # form's own default (512) for it
+        for form, prec, kf in (("fp32", mp.FP32_REANCHOR, k), ("guarded", mp.FP32_GUARDED, 512)):
+            p = ctx.selfjoin(x, m, precision=prec, reanchor_k=kf, diag_lo=lo, diag_hi=hi)
             j = ctx.last_phase_ms()[1]
-            r = er.compare(x, m, segs, p64, p, name == "c3z", K=k)
-            rec[form] = {"cells_per_s": cells / (j * 1e-3),
+            r = er.compare(x, m, segs, p64, p, name == "c3z", K=kf)
+            rec[form] = {"reanchor_k": kf, "cells_per_s": cells / (j * 1e-3),
                          "max_rel_far_from_stretches": r["max_rel_far_from_stretches"],
                          "max_rel_near_stretches": r["max_rel_near_stretches"],
                          "mean_rel": r["mean_rel"], "reference_inaccurate": r["reference_inaccurate"]}

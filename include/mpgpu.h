@@ -80,7 +80,8 @@ size_t mp_selfjoin_scratch_bytes(int64_t n, int64_t m, int precision);
  *   A            n doubles, host or device memory (detected).
  *   excl         exclusion zone; < 0 selects m/4.
  *   precision    mp_precision.
- *   reanchor_k   FP32 form: columns between FP64 re-anchors (0 = 1024).
+ *   reanchor_k   FP32 forms: columns between FP64 re-anchors (0 = 1024 for
+ *                MP_PREC_FP32_REANCHOR, 512 for MP_PREC_FP32_GUARDED).
  *   blocklen     FP64 form: the reference's --blocklen (0 = 500); it decides
  *                which cells the reference evaluates with fused operations,
  *                so it is needed for bit-identical values.

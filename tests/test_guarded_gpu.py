@@ -76,3 +76,20 @@ def test_stress_series_within_tolerance(gpu_ctx, K):
                 assert rep["flat_convention_fp32"], rep
             else:
                 assert rep["pseudo_flat_fp32_is_flat_result"], rep
+
+
+def test_default_interval_meets_bound_far_from_stretches(gpu_ctx):
+    """At its default re-anchor interval (reanchor_k = 0 -> 512) the guarded
+    form's distances stay within 1e-4 of the FP64 form's away from the
+    constant stretches, on both stress series and every sampled range; near
+    them as well."""
+    for zero in (False, True):
+        x, m, info = workloads.c3(zero_level=zero)
+        segs = [(s, L) for kind, s, L in info if kind == "flat"]
+        PL = x.size - m + 1
+        for lo, hi in _ranges(PL, m):
+            p64 = gpu_ctx.selfjoin(x, m, precision=mp.FP64, diag_lo=lo, diag_hi=hi)
+            pg = gpu_ctx.selfjoin(x, m, precision=mp.FP32_GUARDED, diag_lo=lo, diag_hi=hi)
+            rep = error_report.compare(x, m, segs, p64, pg, zero, K=512)
+            assert rep["max_rel_far_from_stretches"] <= 1e-4, (zero, lo, hi, rep)
+            assert rep["max_rel_near_stretches"] <= 1e-4, (zero, lo, hi, rep)
