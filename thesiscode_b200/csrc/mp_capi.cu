@@ -550,7 +550,8 @@ int selfjoin_ranges(mp_context* ctx, const double* A, int64_t n, int64_t m, int 
         MP_CUDA(ctx, cudaMemcpyAsync(desc, Ps.data(), sizeof(Fp32TileParams) * Ps.size(),
                                      cudaMemcpyHostToDevice, st));
         MP_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
-        launch_fp32_join<kFp32R>(desc, (int)Ps.size(), ntiles, counter, st);
+        // the guarded form's keys name candidate groups, resolved in FP64 below
+        launch_fp32_join<kFp32R>(desc, (int)Ps.size(), ntiles, counter, st, guarded);
         MP_LAUNCHED(ctx);
         if (guarded) {
             // the same tiles again: the FP64 pass evaluates those the FP32 pass skipped

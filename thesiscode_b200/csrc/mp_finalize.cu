@@ -43,8 +43,10 @@ __global__ void finalize_fp64_kernel(const unsigned long long* __restrict__ kexa
 }
 
 // FP32 form.  key = (ord(u) << 32) | neighbour, min-merged; the initial key
-// encodes u = 1 + 1/m (score -1) with neighbour 0.  refine != 0 recomputes the
-// chosen pair's distance from a centred FP64 dot product.
+// encodes u = 1 + 1/m (score -1) with neighbour 0.  A group key (low word's
+// kFp32GroupBit set) resolves to its candidate with the largest FP64
+// correlation.  refine != 0 recomputes the chosen pair's distance from a
+// centred FP64 dot product; otherwise the distance is the key's FP32 u.
 __global__ void finalize_fp32_kernel(const unsigned long long* __restrict__ key, int64_t PL,
                                      double m, const double* __restrict__ A,
                                      const double* __restrict__ mean,
@@ -61,7 +63,11 @@ __global__ void finalize_fp32_kernel(const unsigned long long* __restrict__ key,
             idx[i] = 0;
             continue;
         }
-        const int64_t j = (int64_t)(k & 0xffffffffull);
+        const unsigned lo = (unsigned)k, hi = (unsigned)(k >> 32);
+        const bool group = (lo & kFp32GroupBit) != 0u;
+        const int64_t j = group ? fp32_pick_neighbour(A, mean, norm, mm, i, (int64_t)(lo & ~kFp32GroupBit),
+                                                      (int)(hi & 7u) + 1)
+                                : (int64_t)lo;
         idx[i] = j;
         if (refine) {
             const double mi = mean[i], mj = mean[j];
@@ -69,7 +75,7 @@ __global__ void finalize_fp32_kernel(const unsigned long long* __restrict__ key,
             for (int64_t t = 0; t < mm; ++t) c = __fma_rn(A[i + t] - mi, A[j + t] - mj, c);
             d2[i] = 2.0 * m * (1.0 - c * norm[i] * norm[j]);
         } else {
-            d2[i] = 2.0 * m * (double)unord_f32((unsigned)(k >> 32));
+            d2[i] = 2.0 * m * (double)unord_f32(group ? ((hi & ~0xffu) | 0x80u) : hi);
         }
     }
 }

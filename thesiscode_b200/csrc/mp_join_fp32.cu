@@ -24,6 +24,13 @@
 //             warp minimum is one REDUX instruction.  Finished rows/columns
 //             are merged into the profile with a 64-bit atomicMin on
 //             (ordered u, neighbour).
+//  group keys (the guarded form) a lane takes plain float minima over its
+//             own cells, and only the lane's results carry the lane number
+//             in their low 8 bits (one tag per row or column, not per cell);
+//             a key then names the winning lane's R adjacent candidate
+//             neighbours, among which the finalisation picks with FP64 dot
+//             products (fp32_pick_neighbour) -- which also removes FP32
+//             ranking noise between adjacent diagonals.
 //
 // Reference semantics kept: strict improvement over the initial score -1
 // (u < 1 + 1/m), NaN never wins (a zero-variance window has nn = NaN).
@@ -73,6 +80,50 @@ __device__ __forceinline__ float tag_key(float u, unsigned tag) {
 __device__ __forceinline__ float untag_value(unsigned bits) {
     return __uint_as_float((bits & ~kTagMask) | 0x80u);
 }
+// u with the lane number in its low 8 bits (group keys: a lane's minima only).
+__device__ __forceinline__ float tag_lane(float u, unsigned lane) {
+    return __uint_as_float((__float_as_uint(u) & ~kTagMask) | lane);
+}
+
+template <bool GROUP>
+__device__ __forceinline__ float lane_min(float v, int lane) {
+    return GROUP ? tag_lane(v, (unsigned)lane) : v;
+}
+
+// Group keys: merges (u, candidates [base, base + count)) unless u is not
+// below the initial score's ulim.
+__device__ __forceinline__ void merge_group(unsigned long long* key, float u, int64_t base,
+                                            int count, unsigned ulim_ord) {
+    const unsigned hi = (ord_f32(u) & ~kTagMask) | 0x80u | (unsigned)(count - 1);
+    if (hi < ulim_ord)
+        atomicMin(key, ((unsigned long long)hi << 32) | kFp32GroupBit | (unsigned long long)base);
+}
+// Row r's minimum over the band, tagged with its lane L: the cells of lane L
+// in row r are (j = r - g, g = gL + a) for a < R with g < g_hi and j >= 0,
+// gL = gb + L*R, i.e. the columns [r - gL - amax, r - gL].  WHOLE: the tile
+// guarantees amax = R - 1 for every lane (see tile_fp32).
+template <int R, bool WHOLE>
+__device__ __forceinline__ void flush_row_group(const Fp32TileParams& P, float v, int64_t r,
+                                                int64_t gb, unsigned ulim_ord) {
+    const unsigned bits = __float_as_uint(v);
+    const float u = untag_value(bits);
+    if (!(u < kInf)) return;  // no cell (kInf or a NaN pattern)
+    const int64_t gL = gb + (int64_t)(bits & kTagMask) * R;
+    const int64_t amax = WHOLE ? (int64_t)R - 1 : min(min((int64_t)R - 1, P.g_hi - 1 - gL), r - gL);
+    merge_group(P.key + r, u, r - gL - amax, (int)amax + 1, ulim_ord);
+}
+// Column j's minimum over the band, tagged with its lane L: the candidates
+// are rows j + gL + a, a < R, on diagonals < g_hi and rows < PL.  WHOLE: the
+// tile guarantees all R of them for every lane.
+template <int R, bool WHOLE>
+__device__ __forceinline__ void flush_col_group(const Fp32TileParams& P, unsigned bits, int64_t j,
+                                                int64_t gb, unsigned ulim_ord) {
+    const float u = untag_value(bits);
+    if (!(u < kInf)) return;
+    const int64_t gL = gb + (int64_t)(bits & kTagMask) * R;
+    const int64_t cnt = WHOLE ? (int64_t)R : min(min((int64_t)R, P.g_hi - gL), P.PL - j - gL);
+    merge_group(P.key + j, u, j + gL, (int)cnt, ulim_ord);
+}
 
 template <int R>
 __device__ __forceinline__ void flush_row(const Fp32TileParams& P, float v, int64_t r,
@@ -96,7 +147,7 @@ __device__ __forceinline__ void flush_row(const Fp32TileParams& P, float v, int6
 // Slow chunks (near the end of a band) mask cells past the diagonal's end:
 // cell (column jr + b, diagonal g0 + d) exists iff d < ghi_rel and
 // jr + b < min(lim0 - d, ncols).
-template <int R, bool FAST, int OFF>
+template <int R, bool FAST, int OFF, bool GROUP>
 __device__ __forceinline__ void chunk_fp32(const char* rbase, const char* cbuf,
                                            RowWin (&win)[R / 2], float2 (&nc2)[R / 2],
                                            float (&acc)[2 * R], const unsigned (&tag)[R],
@@ -128,8 +179,8 @@ __device__ __forceinline__ void chunk_fp32(const char* rbase, const char* cbuf,
                 const float2 u2 = __ffma2_rn(nc2[a], nn2, one2);
                 nc2[a] = __ffma2_rn(lo2(cv), hi2(rv.dfdg), nc2[a]);
                 nc2[a] = __ffma2_rn(lo2(rv.dfdg), hi2(cv), nc2[a]);
-                kb[a] = tag_key(u2.x, tag[a]);
-                kb[a + H] = tag_key(u2.y, tag[a + H]);
+                kb[a] = GROUP ? u2.x : tag_key(u2.x, tag[a]);
+                kb[a + H] = GROUP ? u2.y : tag_key(u2.y, tag[a + H]);
                 if (!FAST) {
                     const int l0 = a < ghi_rel ? min(lim0 - a, ncols) : 0;
                     const int l1 = a + H < ghi_rel ? min(lim0 - a - H, ncols) : 0;
@@ -139,7 +190,8 @@ __device__ __forceinline__ void chunk_fp32(const char* rbase, const char* cbuf,
                 cmin = a == 0 ? fminf(kb[a], kb[a + H]) : fmin3(cmin, kb[a], kb[a + H]);
             }
             acc[(b + OFF) % (2 * R)] = fminf(acc[(b + OFF) % (2 * R)], kb[0]);
-            const int kmin = __reduce_min_sync(kFullMask, __float_as_int(cmin));
+            const int kmin =
+                __reduce_min_sync(kFullMask, __float_as_int(GROUP ? tag_lane(cmin, lane) : cmin));
             colkey = (lane == b + OFF) ? kmin : colkey;
         }
         {
@@ -159,8 +211,8 @@ __device__ __forceinline__ void chunk_fp32(const char* rbase, const char* cbuf,
                 const float2 u2 = __ffma2_rn(nc2[a], nn2, one2);
                 nc2[a] = __ffma2_rn(lo2(cv), hi2(rv.dfdg), nc2[a]);
                 nc2[a] = __ffma2_rn(lo2(rv.dfdg), hi2(cv), nc2[a]);
-                float k0 = tag_key(u2.x, tag[a]);
-                float k1 = tag_key(u2.y, tag[a + H]);
+                float k0 = GROUP ? u2.x : tag_key(u2.x, tag[a]);
+                float k1 = GROUP ? u2.y : tag_key(u2.y, tag[a + H]);
                 if (!FAST) {
                     const int l0 = a < ghi_rel ? min(lim0 - a, ncols) : 0;
                     const int l1 = a + H < ghi_rel ? min(lim0 - a - H, ncols) : 0;
@@ -181,13 +233,14 @@ __device__ __forceinline__ void chunk_fp32(const char* rbase, const char* cbuf,
                         fmin3(acc[(c + a + H + OFF) % (2 * R)], k1, kb[a + H + 1]);
                 cmin = a == 0 ? fminf(k0, k1) : fmin3(cmin, k0, k1);
             }
-            const int kmin = __reduce_min_sync(kFullMask, __float_as_int(cmin));
+            const int kmin =
+                __reduce_min_sync(kFullMask, __float_as_int(GROUP ? tag_lane(cmin, lane) : cmin));
             colkey = (lane == c + OFF) ? kmin : colkey;
         }
     }
 }
 
-template <int R>
+template <int R, bool GROUP>
 __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, int lane, float* ring,
                           char* rring, char* cring) {
     constexpr int H = R / 2;
@@ -201,6 +254,11 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
     // guarded form: tiles touching a hazard window are evaluated in FP64
     if (P.hazard && fp32_tile_hazardous(P, gb, j0, j1, 32 * R)) return;
     const float ulim = (float)(1.0 + 1.0 / (double)P.m);
+    const unsigned ulim_ord = ord_f32(ulim);
+    // group keys: every lane's candidate groups hold all R candidates (its
+    // diagonals lie below g_hi, rows below PL, and columns, j0 >= R - 1, at or
+    // above 0)
+    const bool whole = j0 >= R - 1 && gb + 32 * R <= P.g_hi && j1 + gb + 32 * R <= P.PL;
 
     // cell (column j, diagonal g0 + d) is evaluated iff d < ghi_rel and
     // j - j0 < min(lim0 - d, ncols); every cell of a chunk ending at or
@@ -332,15 +390,15 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
             const bool fast = __all_sync(kFullMask, jh + R <= minlim);
             if (half == 0) {
                 if (fast)
-                    chunk_fp32<R, true, 0>(rbase, cbuf, win, nc2, acc, tag, lim0, ncols, ghi_rel, jh, lane, colkey);
+                    chunk_fp32<R, true, 0, GROUP>(rbase, cbuf, win, nc2, acc, tag, lim0, ncols, ghi_rel, jh, lane, colkey);
                 else
-                    chunk_fp32<R, false, 0>(rbase, cbuf, win, nc2, acc, tag, lim0, ncols, ghi_rel, jh, lane, colkey);
+                    chunk_fp32<R, false, 0, GROUP>(rbase, cbuf, win, nc2, acc, tag, lim0, ncols, ghi_rel, jh, lane, colkey);
             } else {
                 if (fast)
-                    chunk_fp32<R, true, R>(rbase, cbuf + 32 * R, win, nc2, acc, tag, lim0,
+                    chunk_fp32<R, true, R, GROUP>(rbase, cbuf + 32 * R, win, nc2, acc, tag, lim0,
                                            ncols, ghi_rel, jh, lane, colkey);
                 else
-                    chunk_fp32<R, false, R>(rbase, cbuf + 32 * R, win, nc2, acc, tag,
+                    chunk_fp32<R, false, R, GROUP>(rbase, cbuf + 32 * R, win, nc2, acc, tag,
                                             lim0, ncols, ghi_rel, jh, lane, colkey);
             }
             // this chunk's lower half (rows jh + g0 + [0, R)) is final for the lane
@@ -349,10 +407,10 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
 #pragma unroll
             for (int v = 0; v < R / 4; ++v) {
                 float4 t = rv4[v];
-                t.x = fminf(t.x, acc[(4 * v + 0 + half * R) % (2 * R)]);
-                t.y = fminf(t.y, acc[(4 * v + 1 + half * R) % (2 * R)]);
-                t.z = fminf(t.z, acc[(4 * v + 2 + half * R) % (2 * R)]);
-                t.w = fminf(t.w, acc[(4 * v + 3 + half * R) % (2 * R)]);
+                t.x = fminf(t.x, lane_min<GROUP>(acc[(4 * v + 0 + half * R) % (2 * R)], lane));
+                t.y = fminf(t.y, lane_min<GROUP>(acc[(4 * v + 1 + half * R) % (2 * R)], lane));
+                t.z = fminf(t.z, lane_min<GROUP>(acc[(4 * v + 2 + half * R) % (2 * R)], lane));
+                t.w = fminf(t.w, lane_min<GROUP>(acc[(4 * v + 3 + half * R) % (2 * R)], lane));
                 rv4[v] = t;
             }
             // lane l's next merge reads the chunk lane l + 1 has just written
@@ -363,20 +421,36 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
         __syncwarp();
         // columns jr + [0, 2R): one per lane
         if (lane < 2 * R) {
-            const unsigned bits = (unsigned)colkey;
-            const float u = untag_value(bits);
-            if (u < ulim) {
-                const unsigned t = bits & kTagMask;
-                const int64_t j = j0 + jr + lane;
-                const int64_t q = j + gb + (int64_t)(t >> 3) * R + (t & 7u);
-                atomicMin(P.key + j, ((unsigned long long)ord_f32(u) << 32) | (unsigned long long)q);
+            if constexpr (GROUP) {
+                // rows jr + [0, 2R) of the tile have met every lane: flush, free
+                const int c = jr / R + (lane >> 3);
+                const int e = (c % RK_CHUNKS) * kRowStride + (lane & (R - 1));
+                const float v = ring[e];
+                ring[e] = kInf;
+                const int64_t j = j0 + jr + lane, r = j0 + gb + jr + lane;
+                if (whole) {
+                    flush_col_group<R, true>(P, (unsigned)colkey, j, gb, ulim_ord);
+                    flush_row_group<R, true>(P, v, r, gb, ulim_ord);
+                } else {
+                    flush_col_group<R, false>(P, (unsigned)colkey, j, gb, ulim_ord);
+                    flush_row_group<R, false>(P, v, r, gb, ulim_ord);
+                }
+            } else {
+                const unsigned bits = (unsigned)colkey;
+                const float u = untag_value(bits);
+                if (u < ulim) {
+                    const unsigned t = bits & kTagMask;
+                    const int64_t j = j0 + jr + lane;
+                    const int64_t q = j + gb + (int64_t)(t >> 3) * R + (t & 7u);
+                    atomicMin(P.key + j, ((unsigned long long)ord_f32(u) << 32) | (unsigned long long)q);
+                }
+                // rows jr + [0, 2R) of the tile have met every lane: flush, free
+                const int c = jr / R + (lane >> 3);
+                const int e = (c % RK_CHUNKS) * kRowStride + (lane & (R - 1));
+                const float v = ring[e];
+                ring[e] = kInf;
+                flush_row<R>(P, v, j0 + gb + jr + lane, gb, ulim);
             }
-            // rows jr + [0, 2R) of the tile have met every lane: flush, free
-            const int c = jr / R + (lane >> 3);
-            const int e = (c % RK_CHUNKS) * kRowStride + (lane & (R - 1));
-            const float v = ring[e];
-            ring[e] = kInf;
-            flush_row<R>(P, v, j0 + gb + jr + lane, gb, ulim);
         }
         rec_store(rring, fill + (lane >> 1), lane & 1, nrow);
         *reinterpret_cast<uint4*>(cring + (cb ^ 1) * 64 * R + 16 * lane) = ncol;
@@ -389,15 +463,18 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
     {
         float* base = ring + kslot * kRowStride;
 #pragma unroll
-        for (int k = 0; k < R - 1; ++k) base[k] = fminf(base[k], acc[k]);
+        for (int k = 0; k < R - 1; ++k) base[k] = fminf(base[k], lane_min<GROUP>(acc[k], lane));
     }
     __syncwarp();
     const int cend = jr / R;
     for (int e = lane; e < RK_CHUNKS * R; e += 32) {
         const int cs = e / R;
         const int rel = (cs - cend % RK_CHUNKS + RK_CHUNKS) % RK_CHUNKS;
-        flush_row<R>(P, ring[cs * kRowStride + e % R], j0 + gb + (int64_t)(cend + rel) * R + (e % R),
-                     gb, ulim);
+        const int64_t r = j0 + gb + (int64_t)(cend + rel) * R + (e % R);
+        if constexpr (GROUP)
+            flush_row_group<R, false>(P, ring[cs * kRowStride + e % R], r, gb, ulim_ord);
+        else
+            flush_row<R>(P, ring[cs * kRowStride + e % R], r, gb, ulim);
     }
     __syncwarp();
 }
@@ -414,7 +491,7 @@ constexpr int fp32_smem_bytes() {
 #define MPGPU_FP32_MIN_BLOCKS 3  // 3 x 4 warps per SM (measured best of 2, 3, 4)
 #endif
 
-template <int R>
+template <int R, bool GROUP>
 __global__ void __launch_bounds__(32 * kFp32WarpsPerBlock, MPGPU_FP32_MIN_BLOCKS)
     fp32_join_kernel(const Fp32TileParams* __restrict__ series, int nseries, int64_t total,
                      unsigned long long* __restrict__ counter) {
@@ -446,7 +523,7 @@ __global__ void __launch_bounds__(32 * kFp32WarpsPerBlock, MPGPU_FP32_MIN_BLOCKS
         // one band, so tiles running together touch disjoint columns and rows
         int64_t band, seg;
         if (fp32_tile_of(P, tt - P.tile_begin + P.tile_skip, 32 * R, band, seg))
-            tile_fp32<R>(P, band, seg, lane, ring, rring, cring);
+            tile_fp32<R, GROUP>(P, band, seg, lane, ring, rring, cring);
     }
 }
 
@@ -471,13 +548,15 @@ void fp32_tile_plan(int64_t PL, int64_t g_lo, int64_t g_hi, int64_t K, int R, in
 
 template <int R>
 void configure_fp32_join() {
-    cudaFuncSetAttribute(fp32_join_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(fp32_join_kernel<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         fp32_smem_bytes<R>());
+    cudaFuncSetAttribute(fp32_join_kernel<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          fp32_smem_bytes<R>());
 }
 
 template <int R>
 void launch_fp32_join(const Fp32TileParams* series_dev, int nseries, int64_t total,
-                      unsigned long long* counter, cudaStream_t s) {
+                      unsigned long long* counter, cudaStream_t s, bool group) {
     // the shared-memory limit is a per-device attribute; setting it is
     // idempotent, so concurrent first launches (server threads) are harmless
     static std::atomic<unsigned long long> configured{0};
@@ -490,13 +569,16 @@ void launch_fp32_join(const Fp32TileParams* series_dev, int nseries, int64_t tot
     }
     const int64_t want = (total + kFp32WarpsPerBlock - 1) / kFp32WarpsPerBlock;
     const int64_t blocks = std::min<int64_t>(want, (int64_t)sm_count() * MPGPU_FP32_MIN_BLOCKS);
-    if (blocks > 0)
-        fp32_join_kernel<R><<<(unsigned)blocks, 32 * kFp32WarpsPerBlock, fp32_smem_bytes<R>(), s>>>(
+    if (blocks > 0 && group)
+        fp32_join_kernel<R, true><<<(unsigned)blocks, 32 * kFp32WarpsPerBlock, fp32_smem_bytes<R>(), s>>>(
             series_dev, nseries, total, counter);
+    else if (blocks > 0)
+        fp32_join_kernel<R, false><<<(unsigned)blocks, 32 * kFp32WarpsPerBlock, fp32_smem_bytes<R>(),
+                                     s>>>(series_dev, nseries, total, counter);
 }
 
 template void launch_fp32_join<8>(const Fp32TileParams*, int, int64_t, unsigned long long*,
-                                  cudaStream_t);
+                                  cudaStream_t, bool);
 template void configure_fp32_join<8>();
 
 }  // namespace mpgpu

@@ -102,7 +102,7 @@ struct Fp32TileParams {
     int64_t seg_per_pair;  // tiles per band pair (k, nbands-1-k), max over pairs
     int64_t tile_begin;    // first tile of this series in the launch
     int64_t tile_skip;     // local tile that launch tile tile_begin stands for (0: all)
-    unsigned long long* key;  // [PL] (ordered u << 32 | neighbour), min-merged
+    unsigned long long* key;  // [PL] (ordered u << 32 | neighbour or group), min-merged
     // Guarded form only (all null otherwise): hazard[w] = number of hazard
     // windows among [0, w) (PL + 1 entries); FP64 inverse norms and
     // recurrence terms for the FP64 tiles.
@@ -142,12 +142,73 @@ __device__ __forceinline__ bool fp32_tile_hazardous(const Fp32TileParams& P, int
     const int64_t rs = min(j0 + gb, P.PL), re = min(j1 + gb + span, P.PL);
     return (P.hazard[j1] - P.hazard[j0]) > 0 || (P.hazard[re] - P.hazard[rs]) > 0;
 }
+
+// FP32 profile keys, min-merged: (ordered u << 32) | neighbour.  With group
+// keys (the guarded form) the tile kernel finds a minimum's lane but not which
+// of the lane's R diagonals holds it, so its keys name a group of adjacent
+// candidate neighbours instead: bit 31 of the low word set, the group's first
+// candidate in bits 0..30, and (count - 1) in the low 3 bits of the high word
+// -- below the form's 2^-15 resolution of u, which keeps 0x80 in the low byte
+// of u's pattern.  Keys with bit 31 clear (FP64 tiles, exact pairs, the
+// initial key) name the neighbour itself.
+constexpr unsigned kFp32GroupBit = 0x80000000u;
+// The candidate among [base, base + count) (count <= 8) whose window has the
+// largest centred FP64 correlation with window i, ties to the smaller index;
+// NaN (flat) candidates never win.  A, mean and norm (inverse centred norms)
+// as in the tile kernel; A holds at least 7 values of padding past the series.
+// About 8m FMAs.
+__device__ inline int64_t fp32_pick_neighbour(const double* A, const double* mean,
+                                              const double* norm, int64_t m, int64_t i,
+                                              int64_t base, int count) {
+    double c[8], w[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) c[a] = 0.0;
+    const double mi = mean[i];
+    double sx = 0.0;
+#pragma unroll
+    for (int a = 0; a < 7; ++a) w[a] = A[base + a];
+    int64_t t = 0;
+    for (; t + 8 <= m; t += 8) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            w[(k + 7) % 8] = A[base + t + k + 7];
+            const double x = A[i + t + k] - mi;
+            sx += x;
+#pragma unroll
+            for (int a = 0; a < 8; ++a) c[a] = __fma_rn(x, w[(k + a) % 8], c[a]);
+        }
+    }
+    for (; t < m; ++t) {
+        const double x = A[i + t] - mi;
+        sx += x;
+#pragma unroll
+        for (int a = 0; a < 8; ++a) c[a] = __fma_rn(x, A[base + t + a], c[a]);
+    }
+    // sum_t x_t (A[q+t] - mean_q) = c - mean_q * sum_t x_t; the common factor
+    // norm[i] > 0 does not change the ranking
+    int64_t best = base;
+    double bs = -__builtin_huge_val();
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        if (a < count) {
+            const int64_t q = base + a;
+            const double s = (c[a] - mean[q] * sx) * norm[q];
+            if (s > bs) {
+                bs = s;
+                best = q;
+            }
+        }
+    }
+    return best;
+}
 #endif
 // Persistent launch over `nseries` descriptors (device array) holding `total`
 // tiles; warps take tiles from *counter (zeroed by the caller beforehand).
+// group: the keys name candidate groups (see kFp32GroupBit) instead of
+// neighbours, which the finalisation resolves in FP64.
 template <int R>
 void launch_fp32_join(const Fp32TileParams* series_dev, int nseries, int64_t total,
-                      unsigned long long* counter, cudaStream_t s);
+                      unsigned long long* counter, cudaStream_t s, bool group = false);
 template <int R>
 void configure_fp32_join();
 // Guarded form (mp_guard.cu): hazard windows and the FP64 pass over their tiles.
