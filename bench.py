@@ -531,7 +531,7 @@ def run_ours(args, world):
     roofline = {
         "bound": "fp32-fma-pipe (CUDA cores; no tensor-core or HBM bound)",
         "achieved": achieved, "peak": peak32, "unit": "TFLOP/s", "frac": achieved / peak32,
-        "traffic": traffic, "kernel": "fp32_join_kernel<8>",
+        "traffic": traffic, "kernel": "fp32_join_kernel<8, false>",
         "algorithmic_flops_per_launch": FLOP_PER_CELL * cells_mine,
         "kernel_ms": join_avg_ms,
         "peak_source": "measured in this run: independent-FMA-chain kernel (mp_measure_fma_peak), "

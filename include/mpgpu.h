@@ -183,9 +183,10 @@ int mp_batch_run(mp_batch* b, const void* const* series, double* const* dist2_ou
 
 /*
  * Request server (no counterpart in the reference).  Continuous batching of
- * independent self-joins: requests are admitted in arrival order while fewer
- * than `slots` are admitted and the device memory they need (scratch +
- * resident result) fits in mem_budget_bytes.  A finished profile stays on the
+ * independent self-joins: requests are admitted while fewer than `slots` are
+ * admitted and the device memory they need (scratch + resident result) fits
+ * in mem_budget_bytes, the waiting request with the fewest cells first (a
+ * request that has waited 2 s goes before any other, so none starves).  A finished profile stays on the
  * device until mp_server_collect copies it out (and frees it).  A request
  * larger than the whole budget is rejected (MP_ERR_BUDGET).
  *   MP_PREC_FP32_REANCHOR  one scheduler runs every admitted request as part

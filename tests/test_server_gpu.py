@@ -1,8 +1,8 @@
 """Continuous-batching server: results are identical alone and in the mix
 (requests admitted while others run, overlapping on the device) and equal to
 mp_selfjoin's, a small request that arrives while a large one runs finishes
-first, admission respects the memory budget, oversized requests are
-rejected."""
+first, a free slot goes to the smallest waiting request, admission respects
+the memory budget, oversized requests are rejected."""
 from __future__ import annotations
 
 import time
@@ -88,6 +88,31 @@ def test_small_request_overtakes_a_large_one():
     # finish times, both measured from the large request's submission
     assert dt + rs[2] < 0.5 * rb[2], (dt, rs[2], rb[2])
     assert np.array_equal(rs[1].dist2, alone.dist2) and np.array_equal(rs[1].index, alone.index)
+    srv.close()
+
+
+def test_free_slot_goes_to_the_smallest_waiting_request():
+    """With its one slot taken, the server admits the waiting request with the
+    fewest cells first, not the oldest: a small request submitted after a
+    medium one starts (and finishes) before it."""
+    big = workloads.random_walk(1_048_576, 21)
+    mid = workloads.random_walk(300_000, 22)
+    small = workloads.random_walk(20_000, 23)
+    srv = mp.Server(0, 8 << 30, slots=1)
+    tb, rc = srv.submit(big, 128)
+    assert rc == mp.MP_OK
+    tm, rc = srv.submit(mid, 128)
+    assert rc == mp.MP_OK
+    ts, rc = srv.submit(small, 64)
+    assert rc == mp.MP_OK
+    assert not srv.done(tb)
+    rb = srv.collect(tb, want_profile=False)
+    rm = srv.collect(tm, want_profile=False)
+    rs = srv.collect(ts)
+    assert rb[0] == rm[0] == rs[0] == mp.MP_OK
+    # queue time = submission to start; the small one was submitted last
+    assert rs[3] < rm[3], (rs[3], rm[3])
+    assert rs[2] < rm[2], (rs[2], rm[2])
     srv.close()
 
 

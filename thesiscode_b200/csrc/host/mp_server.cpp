@@ -1,8 +1,10 @@
 // Self-join request server: continuous batching of independent self-joins.
 //
-// Requests are admitted in arrival order as soon as the server has a free
-// slot and the device memory they need (scratch + their resident result) fits
-// in its budget.  A finished profile stays in device memory until the client
+// Requests are admitted as soon as the server has a free slot and the device
+// memory they need (scratch + their resident result) fits in its budget: the
+// waiting request with the fewest cells first, so that under load a small
+// request does not queue behind large ones for a slot, except that a request
+// that has waited kAgeLimitS goes before any other, so none starves.  A finished profile stays in device memory until the client
 // collects it, and its memory counts against the budget until then.  A request
 // larger than the whole budget is rejected at submission.  No counterpart in
 // the reference (one join per process there).
@@ -43,6 +45,7 @@ struct Request {
     int64_t id = 0;
     std::vector<double> series;
     int64_t m = 0, PL = 0;
+    double cells = 0.0;    // cells of the join (the admission order)
     size_t need = 0;       // device bytes while running: scratch + resident result
     size_t accounted = 0;  // bytes of this request currently counted in in_use
     Clock::time_point submitted, started, finished;
@@ -63,7 +66,7 @@ struct mp_server {
     std::mutex mu;
     std::condition_variable cv_work;  // workers wait for admissions
     std::condition_variable cv_done;  // clients wait for completions
-    std::deque<int64_t> waiting;      // submitted, not admitted (FIFO)
+    std::deque<int64_t> waiting;      // submitted, not admitted (arrival order)
     std::deque<int64_t> admitted;     // admitted, not started
     std::unordered_map<int64_t, std::unique_ptr<Request>> reqs;
     size_t in_use = 0;  // bytes of admitted + resident requests
@@ -91,13 +94,31 @@ double cells_of(int64_t n, int64_t m) {
     return L * (L + 1) / 2;
 }
 
-// Moves waiting requests to `admitted` while slots and memory allow (FIFO:
-// the head blocks the queue, so a large request is never starved).
+// A waiting request that has waited this long is admitted before any other.
+constexpr double kAgeLimitS = 2.0;
+
+// Moves waiting requests to `admitted` while slots and memory allow.  The
+// oldest request goes first once it has waited kAgeLimitS (and while it does
+// not fit the memory left, nothing else is admitted); otherwise the one with
+// the fewest cells among those that fit (ties: arrival order).
 void admit_locked(mp_server* s) {
+    const Clock::time_point now = Clock::now();
     while (!s->waiting.empty() && s->free_slots > 0) {
-        Request* r = s->reqs[s->waiting.front()].get();
-        if (s->in_use + r->need > s->budget && s->in_use > 0) break;
-        s->waiting.pop_front();
+        auto fits = [&](const Request* q) { return s->in_use + q->need <= s->budget || s->in_use == 0; };
+        auto pick = s->waiting.begin();
+        Request* head = s->reqs[*pick].get();
+        if (std::chrono::duration<double>(now - head->submitted).count() >= kAgeLimitS) {
+            if (!fits(head)) break;
+        } else {
+            pick = s->waiting.end();
+            for (auto it = s->waiting.begin(); it != s->waiting.end(); ++it) {
+                const Request* q = s->reqs[*it].get();
+                if (fits(q) && (pick == s->waiting.end() || q->cells < s->reqs[*pick]->cells)) pick = it;
+            }
+            if (pick == s->waiting.end()) break;
+        }
+        Request* r = s->reqs[*pick].get();
+        s->waiting.erase(pick);
         s->in_use += r->need;
         r->accounted = r->need;
         --s->free_slots;
@@ -404,6 +425,7 @@ int mp_server_submit(mp_server* s, const double* A, int64_t n, int64_t m, int64_
     r->series.assign(A, A + n);
     r->m = m;
     r->PL = n - m + 1;
+    r->cells = cells_of(n, m);
     r->need = s->epochs ? mpgpu::serve_scratch_bytes(n, m) + mpgpu::serve_result_bytes(n, m)
                         : mp_selfjoin_scratch_bytes(n, m, s->precision) + result_bytes(n - m + 1);
     r->submitted = Clock::now();
