@@ -446,10 +446,11 @@ int selfjoin_ranges(mp_context* ctx, const double* A, int64_t n, int64_t m, int 
 
     // ---- FP32 re-anchored form ----------------------------------------------
     const bool guarded = precision == MP_PREC_FP32_GUARDED;
-    // The guarded form reports the exact distance of the pair the FP32 pass
-    // chose, so its error far from hazards is the FP32 selection error (two
-    // cells' drift): on the c3 stress series (m = 1024) 1.04e-4 at K = 1024,
-    // 6.7e-5 at K = 512.  It therefore defaults to the shorter interval.
+    // The guarded form reports the exact distance of the pair it chose, so its
+    // error far from hazards is the FP32 selection error (two cells' drift)
+    // between candidates more than kPickSpan diagonals apart: on the full c3
+    // stress series (m = 1024) 8.8e-5 at K = 1024, 6.5e-5 at K = 512.  It
+    // defaults to the shorter interval for the margin.
     const int64_t K = reanchor_interval(reanchor_k > 0 ? reanchor_k : (guarded ? kGuardedReanchorK : 0),
                                         kFp32R);
     rc = reserve(ctx, fp32_scratch(n, m, !o_dev, ranges.size()) + (guarded ? guard_scratch(n, m) : 0));
@@ -594,9 +595,13 @@ int selfjoin_ranges(mp_context* ctx, const double* A, int64_t n, int64_t m, int 
         MP_CUDA(ctx, cudaStreamSynchronize(st));
     }
     mark(ctx, 2, st);
-    // guarded form: the chosen pair's distance from a centred FP64 dot product
-    finalize_fp32_kernel<<<grid_for(PL), kThreads, 0, st>>>(key, PL, (double)m, Apad, mean, norm,
-                                                            guarded ? 1 : 0, d2, ix);
+    if (guarded)  // group keys; the chosen pair's distance from a centred FP64 dot product
+        finalize_fp32_guarded_kernel<<<grid_for(PL), kThreads, 0, st>>>(
+            key, PL, (double)m, Apad, mean, norm, ranges.empty() ? 0 : ranges[0].lo,
+            ranges.empty() ? 0 : ranges[0].hi, d2, ix);
+    else
+        finalize_fp32_kernel<<<grid_for(PL), kThreads, 0, st>>>(key, PL, (double)m, Apad, mean, norm,
+                                                                0, d2, ix);
     MP_LAUNCHED(ctx);
     mark(ctx, 3, st);
     if (!o_dev) {

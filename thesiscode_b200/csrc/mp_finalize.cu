@@ -43,10 +43,8 @@ __global__ void finalize_fp64_kernel(const unsigned long long* __restrict__ kexa
 }
 
 // FP32 form.  key = (ord(u) << 32) | neighbour, min-merged; the initial key
-// encodes u = 1 + 1/m (score -1) with neighbour 0.  A group key (low word's
-// kFp32GroupBit set) resolves to its candidate with the largest FP64
-// correlation.  refine != 0 recomputes the chosen pair's distance from a
-// centred FP64 dot product; otherwise the distance is the key's FP32 u.
+// encodes u = 1 + 1/m (score -1) with neighbour 0.  refine != 0 recomputes the
+// chosen pair's distance from a centred FP64 dot product.
 __global__ void finalize_fp32_kernel(const unsigned long long* __restrict__ key, int64_t PL,
                                      double m, const double* __restrict__ A,
                                      const double* __restrict__ mean,
@@ -63,11 +61,7 @@ __global__ void finalize_fp32_kernel(const unsigned long long* __restrict__ key,
             idx[i] = 0;
             continue;
         }
-        const unsigned lo = (unsigned)k, hi = (unsigned)(k >> 32);
-        const bool group = (lo & kFp32GroupBit) != 0u;
-        const int64_t j = group ? fp32_pick_neighbour(A, mean, norm, mm, i, (int64_t)(lo & ~kFp32GroupBit),
-                                                      (int)(hi & 7u) + 1)
-                                : (int64_t)lo;
+        const int64_t j = (int64_t)(k & 0xffffffffull);
         idx[i] = j;
         if (refine) {
             const double mi = mean[i], mj = mean[j];
@@ -75,8 +69,46 @@ __global__ void finalize_fp32_kernel(const unsigned long long* __restrict__ key,
             for (int64_t t = 0; t < mm; ++t) c = __fma_rn(A[i + t] - mi, A[j + t] - mj, c);
             d2[i] = 2.0 * m * (1.0 - c * norm[i] * norm[j]);
         } else {
-            d2[i] = 2.0 * m * (double)unord_f32(group ? ((hi & ~0xffu) | 0x80u) : hi);
+            d2[i] = 2.0 * m * (double)unord_f32((unsigned)(k >> 32));
         }
+    }
+}
+
+// Guarded FP32 form: keys as finalize_fp32_kernel's, except that the FP32
+// pass's keys name candidate groups (kFp32GroupBit); each resolves to the
+// best of its candidates and kPickSpan more on each side, in FP64
+// (fp32_pick_neighbour), within the join's diagonals [g_lo, g_hi).  Every
+// distance is the chosen pair's, from a centred FP64 dot product.
+__global__ void finalize_fp32_guarded_kernel(const unsigned long long* __restrict__ key, int64_t PL,
+                                             double m, const double* __restrict__ A,
+                                             const double* __restrict__ mean,
+                                             const double* __restrict__ norm, int64_t g_lo,
+                                             int64_t g_hi, double* __restrict__ d2,
+                                             int64_t* __restrict__ idx) {
+    const float ulim = (float)(1.0 + 1.0 / m);
+    const unsigned long long init = (unsigned long long)ord_f32(ulim) << 32;
+    const int64_t mm = (int64_t)m;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < PL;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned long long k = key[i];
+        if (k >= init) {
+            d2[i] = 2.0 * m + 2.0;
+            idx[i] = 0;
+            continue;
+        }
+        const unsigned lo = (unsigned)k;
+        int64_t j = (int64_t)(lo & ~kFp32GroupBit);
+        if (lo & kFp32GroupBit) {
+            const int count = (int)((unsigned)(k >> 32) & 7u) + 1;
+            const int64_t q = fp32_pick_neighbour(A, mean, norm, mm, PL, g_lo, g_hi, i, j - kPickSpan,
+                                                  count + 2 * kPickSpan);
+            if (q >= 0) j = q;
+        }
+        idx[i] = j;
+        const double mi = mean[i], mj = mean[j];
+        double c = 0.0;
+        for (int64_t t = 0; t < mm; ++t) c = __fma_rn(A[i + t] - mi, A[j + t] - mj, c);
+        d2[i] = 2.0 * m * (1.0 - c * norm[i] * norm[j]);
     }
 }
 

@@ -152,49 +152,60 @@ __device__ __forceinline__ bool fp32_tile_hazardous(const Fp32TileParams& P, int
 // of u's pattern.  Keys with bit 31 clear (FP64 tiles, exact pairs, the
 // initial key) name the neighbour itself.
 constexpr unsigned kFp32GroupBit = 0x80000000u;
-// The candidate among [base, base + count) (count <= 8) whose window has the
-// largest centred FP64 correlation with window i, ties to the smaller index;
-// NaN (flat) candidates never win.  A, mean and norm (inverse centred norms)
-// as in the tile kernel; A holds at least 7 values of padding past the series.
-// About 8m FMAs.
+// A group key is resolved among its candidates and kPickSpan more on each
+// side (FP32 ranking noise between adjacent diagonals does not stop at a
+// group's edge): of the candidates q in [lo, lo + n) (n <= kPickSlots) that
+// are partners of window i in the join (0 <= q < PL, g_lo <= |i - q| < g_hi),
+// the one whose window has the largest centred FP64 correlation with window
+// i, ties to the smaller index; NaN (flat) candidates never win; -1 when none
+// qualifies.  A, mean and norm (inverse centred norms) as in the tile kernel;
+// A holds at least kPickSlots - 1 values of padding past the series.  About
+// kPickSlots * m FMAs.
+constexpr int kPickSpan = 4;
+constexpr int kPickSlots = 8 + 2 * kPickSpan;
 __device__ inline int64_t fp32_pick_neighbour(const double* A, const double* mean,
-                                              const double* norm, int64_t m, int64_t i,
-                                              int64_t base, int count) {
-    double c[8], w[8];
+                                              const double* norm, int64_t m, int64_t PL,
+                                              int64_t g_lo, int64_t g_hi, int64_t i, int64_t lo,
+                                              int n) {
+    constexpr int W = kPickSlots;
+    const int64_t hi = min(lo + (int64_t)n, PL);
+    lo = max(lo, (int64_t)0);
+    double c[W], w[W];
 #pragma unroll
-    for (int a = 0; a < 8; ++a) c[a] = 0.0;
+    for (int a = 0; a < W; ++a) c[a] = 0.0;
     const double mi = mean[i];
     double sx = 0.0;
 #pragma unroll
-    for (int a = 0; a < 7; ++a) w[a] = A[base + a];
+    for (int a = 0; a < W - 1; ++a) w[a] = A[lo + a];
     int64_t t = 0;
-    for (; t + 8 <= m; t += 8) {
+    for (; t + W <= m; t += W) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            w[(k + 7) % 8] = A[base + t + k + 7];
+        for (int k = 0; k < W; ++k) {
+            w[(k + W - 1) % W] = A[lo + t + k + W - 1];
             const double x = A[i + t + k] - mi;
             sx += x;
 #pragma unroll
-            for (int a = 0; a < 8; ++a) c[a] = __fma_rn(x, w[(k + a) % 8], c[a]);
+            for (int a = 0; a < W; ++a) c[a] = __fma_rn(x, w[(k + a) % W], c[a]);
         }
     }
     for (; t < m; ++t) {
         const double x = A[i + t] - mi;
         sx += x;
 #pragma unroll
-        for (int a = 0; a < 8; ++a) c[a] = __fma_rn(x, A[base + t + a], c[a]);
+        for (int a = 0; a < W; ++a) c[a] = __fma_rn(x, A[lo + t + a], c[a]);
     }
     // sum_t x_t (A[q+t] - mean_q) = c - mean_q * sum_t x_t; the common factor
     // norm[i] > 0 does not change the ranking
-    int64_t best = base;
+    int64_t best = -1;
     double bs = -__builtin_huge_val();
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-        if (a < count) {
-            const int64_t q = base + a;
-            const double s = (c[a] - mean[q] * sx) * norm[q];
-            if (s > bs) {
-                bs = s;
+    for (int a = 0; a < W; ++a) {
+        const int64_t q = lo + a;
+        const int64_t g = q > i ? q - i : i - q;
+        if (q < hi && g >= g_lo && g < g_hi) {
+            const double sc = (c[a] - mean[q] * sx) * norm[q];
+            if (sc > bs) {
+                bs = sc;
                 best = q;
             }
         }
@@ -324,6 +335,9 @@ __global__ void finalize_fp64_kernel(const unsigned long long* kexact, const uns
 __global__ void finalize_fp32_kernel(const unsigned long long* key, int64_t PL, double m,
                                      const double* A, const double* mean, const double* norm,
                                      int refine, double* d2, int64_t* idx);
+__global__ void finalize_fp32_guarded_kernel(const unsigned long long* key, int64_t PL, double m,
+                                             const double* A, const double* mean, const double* norm,
+                                             int64_t g_lo, int64_t g_hi, double* d2, int64_t* idx);
 __global__ void block_keys_init_kernel(const double* prof, int64_t count, unsigned long long* kexact,
                                        unsigned long long* kidx);
 __global__ void block_finalize_kernel(const unsigned long long* kexact, const unsigned long long* kidx,
