@@ -74,6 +74,13 @@ constexpr int kAnchorChunk = 512;
 static_assert(8 * (kAnchorChunk + (32 * 8 + kAnchorChunk) * 9 / 8) <= kRecRingBytes,
               "anchor staging fits the record ring");
 
+// 16-byte copy global -> shared that completes asynchronously (cp.async.cg:
+// cached in L2 only); both addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async16(char* dst_smem, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
 __device__ __forceinline__ float tag_key(float u, unsigned tag) {
     return __uint_as_float((__float_as_uint(u) & ~kTagMask) | tag);
 }
@@ -376,9 +383,18 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
     int kslot = lane;                        // (jr / R + lane) % RK_CHUNKS
     int jr = 0;
     for (; jr < ncols; jr += 2 * R) {
-        // prefetch what the next pair appends: 2R row records and 2R column records
-        const uint4 nrow = __ldg(rsrc + 2 * fill + lane);
-        const uint4 ncol = __ldg(csrc + 2 * (jr + 2 * R) + lane);
+        // prefetch what the next pair appends, 2R row records (ring slots this
+        // pair does not read: the ring holds 33R + H + 2R < kRecRing records
+        // from the pair's first) and 2R column records (the other buffer),
+        // copied straight into shared memory while the pair runs
+        {
+            const int s = rec_slot(fill + (lane >> 1));
+            const uint4* src = rsrc + 2 * fill + lane;
+            cp_async16(rring + rec_off(s) + 16 * (lane & 1), src);
+            if (s < kRecMirror) cp_async16(rring + rec_off(s + kRecRing) + 16 * (lane & 1), src);
+            cp_async16(cring + (cb ^ 1) * 64 * R + 16 * lane, csrc + 2 * (jr + 2 * R) + lane);
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+        }
         int colkey = 0x7fffffff;
         const char* cbuf = cring + cb * 64 * R;
 #pragma unroll
@@ -452,8 +468,7 @@ __device__ void tile_fp32(const Fp32TileParams& P, int64_t band, int64_t seg, in
                 flush_row<R>(P, v, j0 + gb + jr + lane, gb, ulim);
             }
         }
-        rec_store(rring, fill + (lane >> 1), lane & 1, nrow);
-        *reinterpret_cast<uint4*>(cring + (cb ^ 1) * 64 * R + 16 * lane) = ncol;
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         cb ^= 1;
         fill += 2 * R;
         __syncwarp();
