@@ -2,7 +2,8 @@
 (requests admitted while others run, overlapping on the device) and equal to
 mp_selfjoin's, a small request that arrives while a large one runs finishes
 first, a free slot goes to the smallest waiting request, admission respects
-the memory budget, oversized requests are rejected."""
+the memory budget, oversized requests are rejected; the FP64 and guarded
+worker modes give mp_selfjoin's results from pool-lent scratch."""
 from __future__ import annotations
 
 import time
@@ -113,6 +114,34 @@ def test_free_slot_goes_to_the_smallest_waiting_request():
     # queue time = submission to start; the small one was submitted last
     assert rs[3] < rm[3], (rs[3], rm[3])
     assert rs[2] < rm[2], (rs[2], rm[2])
+    srv.close()
+
+
+@pytest.mark.parametrize("prec", [mp.FP64, mp.FP32_GUARDED])
+def test_worker_mode_results_and_budget(prec):
+    """FP64 and guarded servers run whole mp_selfjoin calls on worker threads,
+    each lent its scratch from the server's pool: results equal mp_selfjoin's,
+    a budget with room for about one request at a time completes them all, and
+    nothing stays counted once every result is collected."""
+    m = 128
+    xs = [workloads.random_walk(n, 30 + k) for k, n in enumerate((40_000, 60_000, 50_000))]
+    lib = mp.load_library()
+    need = max(lib.mp_selfjoin_scratch_bytes(x.size, m, prec) + 16 * (x.size - m + 1) + 512
+               for x in xs)
+    srv = mp.Server(0, int(need * 1.3), slots=2, precision=prec, reanchor_k=512)
+    ts = []
+    for x in xs:
+        t, rc = srv.submit(x, m)
+        assert rc == mp.MP_OK
+        ts.append(t)
+    res = [srv.collect(t) for t in ts]
+    ctx = mp.Context(0)
+    for x, r in zip(xs, res):
+        assert r[0] == mp.MP_OK
+        want = ctx.selfjoin(x, m, precision=prec, reanchor_k=512)
+        assert np.array_equal(r[1].dist2, want.dist2) and np.array_equal(r[1].index, want.index)
+    ctx.close()
+    assert srv.stats()["bytes_in_use"] == 0
     srv.close()
 
 

@@ -145,14 +145,23 @@ void worker_main(mp_server* s) {
         }
         const int64_t n = (int64_t)r->series.size(), PL = r->PL;
         int rc = ctx ? MP_OK : MP_ERR_NO_DEVICE;
-        if (rc == MP_OK && (cudaMallocAsync((void**)&r->d_d2, 8 * PL, st) != cudaSuccess ||
-                            cudaMallocAsync((void**)&r->d_idx, 8 * PL, st) != cudaSuccess)) {
+        // scratch and result from the server's pool (the request's `need`)
+        const size_t scr = mp_selfjoin_scratch_bytes(n, r->m, s->precision);
+        void* scratch = nullptr;
+        if (rc == MP_OK &&
+            (cudaMallocFromPoolAsync((void**)&r->d_d2, 8 * PL, s->pool, st) != cudaSuccess ||
+             cudaMallocFromPoolAsync((void**)&r->d_idx, 8 * PL, s->pool, st) != cudaSuccess ||
+             cudaMallocFromPoolAsync(&scratch, scr, s->pool, st) != cudaSuccess)) {
             cudaGetLastError();
             rc = MP_ERR_OUT_OF_MEMORY;
         }
-        if (rc == MP_OK)
+        if (rc == MP_OK) {
+            mpgpu::ctx_lend_scratch(ctx, scratch, scr);
             rc = mp_selfjoin(ctx, r->series.data(), n, r->m, -1, s->precision, s->reanchor_k, 0, 0,
                              0, r->d_d2, r->d_idx, st);
+            mpgpu::ctx_lend_scratch(ctx, nullptr, 0);
+        }
+        if (scratch) cudaFreeAsync(scratch, st);
         if (rc != MP_OK) {
             if (r->d_d2) cudaFreeAsync(r->d_d2, st);
             if (r->d_idx) cudaFreeAsync(r->d_idx, st);
@@ -396,21 +405,22 @@ int mp_server_create(int device, size_t mem_budget_bytes, int slots, int precisi
     s->free_slots = slots;
     s->slots = slots;
     s->epochs = precision == MP_PREC_FP32_REANCHOR;
+    // a pool of the server's own that keeps what it has been given (no release
+    // to the driver between requests); the budget bounds it.  Every device
+    // buffer of a request (scratch and result) comes from it.
+    cudaSetDevice(device);
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess) {
+        cudaGetLastError();
+        delete s;
+        return MP_ERR_CUDA;
+    }
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     if (s->epochs) {
-        // a pool of the server's own that keeps what it has been given (no
-        // release to the driver between requests); the budget bounds it
-        cudaSetDevice(device);
-        cudaMemPoolProps props{};
-        props.allocType = cudaMemAllocationTypePinned;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = device;
-        if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess) {
-            cudaGetLastError();
-            delete s;
-            return MP_ERR_CUDA;
-        }
-        uint64_t keep = UINT64_MAX;
-        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
         s->engine = std::thread(engine_main, s);
     } else {
         for (int i = 0; i < slots; ++i) s->workers.emplace_back(worker_main, s);

@@ -17,6 +17,7 @@
 #include "../../include/mpgpu.h"
 #include "mp_common.cuh"
 #include "mp_kernels.h"
+#include "mp_serve.h"
 
 using namespace mpgpu;
 
@@ -27,6 +28,11 @@ struct mp_context {
     int64_t launches = 0;
     void* arena = nullptr;
     size_t arena_bytes = 0;
+    // while a caller's buffer is lent as the scratch (ctx_lend_scratch), the
+    // context's own arena waits here
+    bool lent = false;
+    void* own_arena = nullptr;
+    size_t own_bytes = 0;
     bool timing = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     double phase_ms[3] = {-1.0, -1.0, -1.0};
@@ -36,6 +42,24 @@ struct mp_context {
 namespace mpgpu {
 size_t ctx_budget(const mp_context* ctx) { return ctx ? ctx->budget : 0; }
 int ctx_device(const mp_context* ctx) { return ctx ? ctx->device : 0; }
+void ctx_lend_scratch(mp_context* ctx, void* scratch, size_t bytes) {
+    if (!ctx) return;
+    if (scratch) {
+        if (!ctx->lent) {
+            ctx->own_arena = ctx->arena;
+            ctx->own_bytes = ctx->arena_bytes;
+            ctx->lent = true;
+        }
+        ctx->arena = scratch;
+        ctx->arena_bytes = bytes;
+    } else if (ctx->lent) {
+        ctx->arena = ctx->own_arena;
+        ctx->arena_bytes = ctx->own_bytes;
+        ctx->own_arena = nullptr;
+        ctx->own_bytes = 0;
+        ctx->lent = false;
+    }
+}
 }  // namespace mpgpu
 
 namespace {
@@ -89,6 +113,9 @@ int reserve(mp_context* ctx, size_t bytes) {
         return fail(ctx, MP_ERR_BUDGET, "request needs %zu bytes of device scratch, budget is %zu",
                     bytes, ctx->budget);
     if (bytes <= ctx->arena_bytes) return MP_OK;
+    if (ctx->lent)  // a lent scratch is never replaced
+        return fail(ctx, MP_ERR_BUDGET, "lent scratch holds %zu bytes, the call needs %zu",
+                    ctx->arena_bytes, bytes);
     if (ctx->arena) cudaFree(ctx->arena);
     ctx->arena = nullptr;
     ctx->arena_bytes = 0;
@@ -295,7 +322,8 @@ int mp_context_create(int device, size_t mem_budget_bytes, mp_context** out) {
 int mp_context_destroy(mp_context* ctx) {
     if (!ctx) return MP_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
-    if (ctx->arena) cudaFree(ctx->arena);
+    void* own = ctx->lent ? ctx->own_arena : ctx->arena;
+    if (own) cudaFree(own);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     delete ctx;

@@ -14,7 +14,18 @@
 
 #include <vector>
 
+struct mp_context;
+
 namespace mpgpu {
+
+// Lends ctx the device buffer `scratch` (bytes long) as its scratch for the
+// calls that follow: the context neither uses nor grows its own arena, and a
+// call that needs more than `bytes` fails with MP_ERR_BUDGET.  scratch =
+// nullptr gives the context its own arena back.  The request server's
+// workers lend each request a buffer from the server's pool, so that their
+// scratch is counted in its budget and released without a device-wide
+// synchronisation (mp_capi.cu).
+void ctx_lend_scratch(mp_context* ctx, void* scratch, size_t bytes);
 
 // One admitted request on the device.  All buffers come from the server's
 // stream-ordered memory pool.
