@@ -168,19 +168,31 @@ __device__ __forceinline__ void thr_store(double* tring, int t, double v) {
 }
 
 // The (score, index) selection of one column step: row partials (strict '>',
-// the reference's rule; a partial started at its row's threshold keeps the
-// sentinel index -1 until a cell beats it), then the column's best cell over
+// the reference's rule; a partial started at its row's threshold has no
+// source (RowSrc) until a cell beats it), then the column's best cell over
 // the warp from two REDUX instructions (high, then low word of the ordered
 // score); the lowest winning lane parks (score, row) in the warp's column slot
 // with a predicated store, so no divergent branch splits consecutive steps.
+// Where a lane's 2R - 1 row partials came from: the diagonal offset a < R of
+// the selected cell, as nibble k = a + 1, or 0 while partial k is still its
+// row's threshold (no candidate yet).  One 64-bit register pair instead of
+// 2R - 1 registers.
+struct RowSrc {
+    unsigned long long w;
+    __device__ __forceinline__ int get(int k) const { return (int)((w >> (4 * k)) & 15ull) - 1; }
+    __device__ __forceinline__ void set(int k, int a) {
+        w = (w & ~(15ull << (4 * k))) | ((unsigned long long)(a + 1) << (4 * k));
+    }
+};
 template <int R>
 __device__ __forceinline__ void select_rows(int b, const double (&sc)[R], double (&acc_s)[2 * R - 1],
-                                            int (&acc_a)[2 * R - 1]) {
+                                            RowSrc& acc_a) {
+    static_assert(2 * R - 1 <= 16, "2R - 1 nibbles fit 64 bits");
 #pragma unroll
     for (int a = 0; a < R; ++a) {
         if (sc[a] > acc_s[b + a]) {
             acc_s[b + a] = sc[a];
-            acc_a[b + a] = a;
+            acc_a.set(b + a, a);
         }
     }
 }
@@ -219,7 +231,7 @@ __device__ __forceinline__ void select_column(const Fp64BandParams& P, int b, co
 }
 template <int R>
 __device__ __forceinline__ void select_step(const Fp64BandParams& P, int b, const double (&sc)[R],
-                                            double (&acc_s)[2 * R - 1], int (&acc_a)[2 * R - 1],
+                                            double (&acc_s)[2 * R - 1], RowSrc& acc_a,
                                             int64_t g0, int lane, double* cslot_s, int* cslot_r) {
     select_rows<R>(b, sc, acc_s, acc_a);
     select_column<R>(P, b, sc, g0, lane, cslot_s, cslot_r);
@@ -235,7 +247,7 @@ template <int R, bool FAST>
 __device__ __forceinline__ bool chunk_fp64(const Fp64BandParams& P, int64_t jc, const char* rring,
                                            const char* rbase, int tbase, double4 (&rwin)[R], double (&qt)[R],
                                            const int (&len)[R], const int (&psw)[R],
-                                           double (&acc_s)[2 * R - 1], int (&acc_a)[2 * R - 1],
+                                           double (&acc_s)[2 * R - 1], RowSrc& acc_a,
                                            int64_t g0, int lane, double* cslot_s, int* cslot_r,
                                            const double* cthr, const char* ccur) {
     bool selected = !FAST;
@@ -354,13 +366,12 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
 #pragma unroll
     for (int k = 0; k < R - 1; ++k) rwin[k] = ring_rec(rring + rec_off(rec_slot(lane * R + k)));
     // row partials: slot k holds row g0 + jc + k, starting at the row's
-    // threshold with the sentinel index -1 (no candidate yet)
+    // threshold with no source (no candidate yet)
     double acc_s[2 * R - 1];
-    int acc_a[2 * R - 1];
+    RowSrc acc_a{0ull};
 #pragma unroll
     for (int k = 0; k < 2 * R - 1; ++k) {
         acc_s[k] = tring[thr_off(lane * R + k)];
-        acc_a[k] = -1;
     }
 
     bool sel_prev = false;
@@ -408,9 +419,10 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
             const int base = (int)(((jc / R) + lane) % 32) * R;
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                if (acc_a[k] >= 0 && acc_s[k] > ring_s[base + k]) {
+                const int a = acc_a.get(k);
+                if (a >= 0 && acc_s[k] > ring_s[base + k]) {
                     ring_s[base + k] = acc_s[k];
-                    ring_c[base + k] = (int)(jc + k - acc_a[k]);
+                    ring_c[base + k] = (int)(jc + k - a);
                 }
             }
         }
@@ -426,10 +438,8 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
         }
         __syncwarp();
 #pragma unroll
-        for (int k = 0; k < R - 1; ++k) {
-            acc_s[k] = acc_s[k + R];
-            acc_a[k] = acc_a[k + R];
-        }
+        for (int k = 0; k < R - 1; ++k) acc_s[k] = acc_s[k + R];
+        acc_a.w >>= 4 * R;  // and the new rows' nibbles are 0
         // new rows jc + R + g0 + k start at their thresholds
         if (R == 8) {
             // rows tbase + 8 + k: slot s0 + k with s0 = (tbase + 8) % kRecRing a
@@ -438,13 +448,11 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
 #pragma unroll
             for (int k = R - 1; k < 2 * R - 1; ++k) {
                 acc_s[k] = tb[k + (k >> 3)];
-                acc_a[k] = -1;
             }
         } else {
 #pragma unroll
             for (int k = R - 1; k < 2 * R - 1; ++k) {
                 acc_s[k] = tring[thr_off(tbase + R + k)];
-                acc_a[k] = -1;
             }
         }
     }
@@ -454,9 +462,10 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
     const int base = (int)(((jend / R) + lane) % 32) * R;
 #pragma unroll
     for (int k = 0; k < R - 1; ++k) {
-        if (acc_a[k] >= 0 && acc_s[k] > ring_s[base + k]) {
+        const int a = acc_a.get(k);
+        if (a >= 0 && acc_s[k] > ring_s[base + k]) {
             ring_s[base + k] = acc_s[k];
-            ring_c[base + k] = (int)(jend + k - acc_a[k]);
+            ring_c[base + k] = (int)(jend + k - a);
         }
     }
     __syncwarp();
