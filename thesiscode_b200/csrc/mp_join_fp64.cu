@@ -246,7 +246,7 @@ __device__ __forceinline__ void select_step(const Fp64BandParams& P, int b, cons
 template <int R, bool FAST>
 __device__ __forceinline__ bool chunk_fp64(const Fp64BandParams& P, int64_t jc, const char* rring,
                                            const char* rbase, int tbase, double4 (&rwin)[R], double (&qt)[R],
-                                           const int (&len)[R], const int (&psw)[R],
+                                           const int* lgeo,
                                            double (&acc_s)[2 * R - 1], RowSrc& acc_a,
                                            int64_t g0, int lane, double* cslot_s, int* cslot_r,
                                            const double* cthr, const char* ccur) {
@@ -285,9 +285,9 @@ __device__ __forceinline__ bool chunk_fp64(const Fp64BandParams& P, int64_t jc, 
             for (int a = 0; a < R; ++a) {
                 const double4 rv = rwin[(b + a) % R];
                 double score;
-                if (j < len[a]) {
+                if (j < lgeo[a * 32]) {
                     const double ss = __dmul_rn(rv.z, cv.z);
-                    if (j <= psw[a]) {
+                    if (j <= lgeo[(R + a) * 32]) {
                         const double mm = __dmul_rn(cv.w, rv.w);
                         score = __fma_rn(qt[a], ss, -mm);
                         qt[a] = __fma_rn(-rv.x, cv.x, __fma_rn(rv.y, cv.y, qt[a]));
@@ -312,31 +312,35 @@ template <int R>
 __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band, int lane,
                                           int shard, double* ring_s, int* ring_c, char* rring,
                                           double* cslot_s, int* cslot_r, double* tring,
-                                          double* cthr, char* ccol) {
+                                          double* cthr, char* ccol, int* lgeo) {
     constexpr int RING = 32 * R;
     const int64_t gb = P.g_lo + band * (int64_t)RING;
     const int64_t g0 = gb + (int64_t)lane * R;
     const int64_t jmax = P.Tbase - gb;  // length of the band's longest diagonal
     if (jmax <= 0) return;
 
+    // Per diagonal a of the lane: len = its column count, psw = its last
+    // column of the reference's 4-wide part (-1: none), kept in the lane's
+    // slots of shared memory (lgeo[a*32], lgeo[(R+a)*32]; columns < 2^31,
+    // checked by the host): only the chunks near a diagonal's end read them.
     double qt[R];
-    int len[R], psw[R];  // columns < 2^31 (checked by the host)
     int minpsw = INT32_MAX;
 #pragma unroll
     for (int a = 0; a < R; ++a) {
         const int64_t g = g0 + a;
+        int len = 0, psw = -1;
         if (g < P.g_hi) {
             const int64_t delta = (g - P.blk_origin) % P.B;
             const int64_t T = P.Tbase - (g - delta);
             qt[a] = P.qt0[g - P.g_lo];
-            len[a] = (int)(T - delta);
-            psw[a] = (delta < (P.B & ~3ll)) ? (int)(T - 4 * (delta / 4 + 1)) : -1;
+            len = (int)(T - delta);
+            psw = (delta < (P.B & ~3ll)) ? (int)(T - 4 * (delta / 4 + 1)) : -1;
         } else {
             qt[a] = 0.0;
-            len[a] = 0;
-            psw[a] = -1;
         }
-        minpsw = min(minpsw, psw[a]);
+        lgeo[a * 32] = len;
+        lgeo[(R + a) * 32] = psw;
+        minpsw = min(minpsw, psw);
     }
 
     // ring of row partials, slot = (r - gb) mod RING; column slots of a chunk
@@ -391,10 +395,10 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
         const bool fast = __all_sync(kFullMask, jc + R - 1 <= minpsw);
         bool sel;
         if (fast)
-            sel = chunk_fp64<R, true>(P, jc, rring, rbase, tbase, rwin, qt, len, psw, acc_s, acc_a,
+            sel = chunk_fp64<R, true>(P, jc, rring, rbase, tbase, rwin, qt, lgeo, acc_s, acc_a,
                                       g0, lane, cslot_s, cslot_r, cthr, ccur);
         else
-            sel = chunk_fp64<R, false>(P, jc, rring, rbase, tbase, rwin, qt, len, psw, acc_s, acc_a,
+            sel = chunk_fp64<R, false>(P, jc, rring, rbase, tbase, rwin, qt, lgeo, acc_s, acc_a,
                                        g0, lane, cslot_s, cslot_r, cthr, ccur);
         __syncwarp();
         // the chunk's column maxima (one per column, parked by the winning lane)
@@ -489,7 +493,7 @@ template <int R>
 constexpr int fp64_smem_bytes() {
     return kFp64WarpsPerBlock *
            (kRecRingBytes + 2 * 32 * R + (32 * R + R) * (int)(sizeof(double) + sizeof(int)) +
-            (kThrRingDoubles + R) * (int)sizeof(double));
+            (kThrRingDoubles + R) * (int)sizeof(double) + 2 * R * 32 * (int)sizeof(int));
 }
 
 template <int R>
@@ -514,6 +518,8 @@ __global__ void __launch_bounds__(32 * kFp64WarpsPerBlock) fp64_band_kernel(cons
     int* ring_c = reinterpret_cast<int*>(p) + w * 32 * R;
     p += kW * 32 * R * sizeof(int);
     int* cslot_r = reinterpret_cast<int*>(p) + w * R;
+    p += kW * R * sizeof(int);
+    int* lgeo = reinterpret_cast<int*>(p) + w * 2 * R * 32 + lane;
     // One resident wave of W warps.  Band b (longest first: band lengths fall
     // with b) goes to warp b mod W in even rounds and W-1 - (b mod W) in odd
     // rounds, so every warp's bands add up to nearly the same length -- the
@@ -525,7 +531,7 @@ __global__ void __launch_bounds__(32 * kFp64WarpsPerBlock) fp64_band_kernel(cons
         const int64_t band = r * W + ((r & 1) ? W - 1 - wid : wid);
         if (band >= P.nbands) break;
         band_fp64<R>(P, band, lane, shard, ring_s, ring_c, rring, cslot_s, cslot_r, tring, cthr,
-                     ccol);
+                     ccol, lgeo);
     }
 }
 
