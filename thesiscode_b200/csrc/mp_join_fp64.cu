@@ -131,6 +131,17 @@ __device__ __forceinline__ unsigned step_hits<8>(const double (&sc)[8], const do
     return r;
 }
 
+// Asynchronous copies global -> shared (both addresses aligned to the size):
+// 16 bytes through L2 only, 8 bytes through L1.
+__device__ __forceinline__ void cp_async16(char* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+
 // A threshold as it stands (other warps raise it with atomics meanwhile; any
 // value it has held is a valid lower bound).
 __device__ __forceinline__ double ld_thr(const double* p) {
@@ -380,15 +391,26 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
 
     bool sel_prev = false;
     for (int64_t jc = 0; jc < jmax; jc += R) {
-        uint4 next = make_uint4(0, 0, 0, 0);
-        if (lane < 2 * R) next = __ldg(rsrc + 2 * fill + lane);
-        double tnext = 0.0, cnext = 0.0;  // next rows' and next chunk's column thresholds
-        if (lane < R) {
-            tnext = ld_thr(tsrc + fill + lane);
-            cnext = ld_thr(csrc + jc + R + lane);
+        // Prefetch what the next chunk appends -- R row records and their
+        // rows' thresholds into ring slots this chunk does not read (it reads
+        // rows below fill - 1), R column records and column thresholds into
+        // the other buffers -- copied straight into shared memory while the
+        // chunk runs.  A threshold copied through L1 may be older than the
+        // value in L2; any value it has held is a valid lower bound.
+        if (lane < 2 * R) {
+            const int sr = rec_slot(fill + (lane >> 1));
+            const uint4* src = rsrc + 2 * fill + lane;
+            cp_async16(rring + rec_off(sr) + 16 * (lane & 1), src);
+            if (sr < kRecMirror) cp_async16(rring + rec_off(sr + kRecRing) + 16 * (lane & 1), src);
+            cp_async16(ccol + (cbuf ^ 1) * (32 * R) + 16 * lane, csrc_rec + 2 * (jc + R) + lane);
         }
-        uint4 cnrec = make_uint4(0, 0, 0, 0);  // next chunk's column records
-        if (lane < 2 * R) cnrec = __ldg(csrc_rec + 2 * (jc + R) + lane);
+        if (lane < R) {
+            const int st = (fill + lane) % kRecRing;
+            cp_async8(tring + thr_pos(st), tsrc + fill + lane);
+            if (st < kThrMirror) cp_async8(tring + thr_pos(st + kRecRing), tsrc + fill + lane);
+            cp_async8(cthr + (cbuf ^ 1) * R + lane, csrc + jc + R + lane);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
         const char* ccur = ccol + cbuf * (32 * R);
         const int tbase = (int)jc + lane * R;
         const char* rbase = rring + rec_off(rec_slot(tbase + R - 1));
@@ -396,10 +418,10 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
         bool sel;
         if (fast)
             sel = chunk_fp64<R, true>(P, jc, rring, rbase, tbase, rwin, qt, lgeo, acc_s, acc_a,
-                                      g0, lane, cslot_s, cslot_r, cthr, ccur);
+                                      g0, lane, cslot_s, cslot_r, cthr + cbuf * R, ccur);
         else
             sel = chunk_fp64<R, false>(P, jc, rring, rbase, tbase, rwin, qt, lgeo, acc_s, acc_a,
-                                       g0, lane, cslot_s, cslot_r, cthr, ccur);
+                                       g0, lane, cslot_s, cslot_r, cthr + cbuf * R, ccur);
         __syncwarp();
         // the chunk's column maxima (one per column, parked by the winning lane)
         if (sel && lane < R) {
@@ -409,12 +431,7 @@ __device__ __forceinline__ void band_fp64(const Fp64BandParams& P, int64_t band,
                            jc + cslot_r[lane] + P.row_nb_off);
             cslot_s[lane] = -DBL_MAX;
         }
-        if (lane < 2 * R) rec_store(rring, fill + (lane >> 1), lane & 1, next);
-        if (lane < R) {
-            thr_store(tring, fill + lane, tnext);
-            cthr[lane] = cnext;
-        }
-        if (lane < 2 * R) *reinterpret_cast<uint4*>(ccol + (cbuf ^ 1) * (32 * R) + 16 * lane) = cnrec;
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         cbuf ^= 1;
         fill += R;
         // rows jc + g0 + [0, R) are done for this lane: merge its candidates
@@ -493,7 +510,7 @@ template <int R>
 constexpr int fp64_smem_bytes() {
     return kFp64WarpsPerBlock *
            (kRecRingBytes + 2 * 32 * R + (32 * R + R) * (int)(sizeof(double) + sizeof(int)) +
-            (kThrRingDoubles + R) * (int)sizeof(double) + 2 * R * 32 * (int)sizeof(int));
+            (kThrRingDoubles + 2 * R) * (int)sizeof(double) + 2 * R * 32 * (int)sizeof(int));
 }
 
 template <int R>
@@ -513,8 +530,8 @@ __global__ void __launch_bounds__(32 * kFp64WarpsPerBlock) fp64_band_kernel(cons
     p += kW * 32 * R * sizeof(double);
     double* cslot_s = reinterpret_cast<double*>(p) + w * R;
     p += kW * R * sizeof(double);
-    double* cthr = reinterpret_cast<double*>(p) + w * R;
-    p += kW * R * sizeof(double);
+    double* cthr = reinterpret_cast<double*>(p) + w * 2 * R;  // two buffers of R
+    p += kW * 2 * R * sizeof(double);
     int* ring_c = reinterpret_cast<int*>(p) + w * 32 * R;
     p += kW * 32 * R * sizeof(int);
     int* cslot_r = reinterpret_cast<int*>(p) + w * R;
