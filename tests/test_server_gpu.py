@@ -1,7 +1,8 @@
 """Continuous-batching server: results are identical alone and in the mix
 (requests admitted while others run, overlapping on the device) and equal to
 mp_selfjoin's, a small request that arrives while a large one runs finishes
-first, a free slot goes to the smallest waiting request, admission respects
+first, a free slot goes to the smallest waiting request but none waits more than
+about 2 s for one, admission respects
 the memory budget, oversized requests are rejected; the FP64 and guarded
 worker modes give mp_selfjoin's results from pool-lent scratch."""
 from __future__ import annotations
@@ -114,6 +115,31 @@ def test_free_slot_goes_to_the_smallest_waiting_request():
     # queue time = submission to start; the small one was submitted last
     assert rs[3] < rm[3], (rs[3], rm[3])
     assert rs[2] < rm[2], (rs[2], rm[2])
+    srv.close()
+
+
+def test_waiting_request_goes_first_after_two_seconds():
+    """Shortest-first admission does not starve a larger request: with one
+    slot and small requests always waiting beside it (each would be admitted
+    before it), a medium request is admitted once it has waited 2 s."""
+    small, m_small = workloads.random_walk(20_000, 41), 64
+    mid, m_mid = workloads.random_walk(200_000, 42), 128
+    srv = mp.Server(0, 8 << 30, slots=1)
+    tickets = [srv.submit(small, m_small)[0] for _ in range(32)]
+    tm, rc = srv.submit(mid, m_mid)
+    assert rc == mp.MP_OK
+    t0 = time.perf_counter()
+    while not srv.done(tm) and time.perf_counter() - t0 < 4.0:
+        if srv.stats()["waiting"] < 32:  # keep small requests queued beside it
+            tickets.append(srv.submit(small, m_small)[0])
+        else:
+            time.sleep(0.0002)
+    rm = srv.collect(tm, want_profile=False)
+    rs = [srv.collect(t, want_profile=False) for t in tickets]
+    assert rm[0] == mp.MP_OK and all(r[0] == mp.MP_OK for r in rs)
+    # queue time = submission to start: its 2 s mark plus at most a small request
+    assert 2.0 <= rm[3] < 2.5, rm[3]
+    assert len(tickets) > 64  # small requests kept being admitted before it until then
     srv.close()
 
 
