@@ -20,7 +20,9 @@
 // comes from a server-owned stream-ordered pool, so no allocation or release
 // waits for the device.
 // FP64 and guarded FP32 forms: worker threads, each running whole
-// mp_selfjoin calls on its own stream and context.
+// mp_selfjoin calls on its own stream and context, with each call's scratch
+// and result taken from the same pool (the scratch lent to the context for
+// the call), so the budget counts all of it and nothing waits on cudaFree.
 #include <cuda_runtime.h>
 
 #include <algorithm>
