@@ -60,8 +60,10 @@ __device__ __forceinline__ double4 ring_rec(const char* p) {
 
 // Which parts of a column step need the selection, voted over the warp: bit 0
 // when some lane has a cell above its row partial, bit 1 when some cell is
-// above the column's threshold.  One chain of predicated compares per lane
-// (setp ... .or) and two votes; NaN compares false, so NaN cells never select.
+// above the column's threshold.  Chains of predicated compares per lane
+// (setp ... .or; with R = 8 two chains of 4 per test, interleaved, so the
+// dependent compares are half as deep) and two votes; NaN compares false, so
+// NaN cells never select.
 template <int R>
 __device__ __forceinline__ unsigned step_hits(const double (&sc)[R], const double (&acc)[2 * R - 1],
                                               int b, double tc) {
@@ -102,23 +104,25 @@ __device__ __forceinline__ unsigned step_hits<8>(const double (&sc)[8], const do
                                                  int b, double tc) {
     unsigned r;
     asm volatile(
-        "{\n\t.reg .pred pr, pc, qr, qc;\n\t"
+        "{\n\t.reg .pred pr, pc, pr2, pc2, qr, qc;\n\t"
         "setp.gt.f64 pr, %1, %9;\n\t"
-        "setp.gt.or.f64 pr, %2, %10, pr;\n\t"
-        "setp.gt.or.f64 pr, %3, %11, pr;\n\t"
-        "setp.gt.or.f64 pr, %4, %12, pr;\n\t"
-        "setp.gt.or.f64 pr, %5, %13, pr;\n\t"
-        "setp.gt.or.f64 pr, %6, %14, pr;\n\t"
-        "setp.gt.or.f64 pr, %7, %15, pr;\n\t"
-        "setp.gt.or.f64 pr, %8, %16, pr;\n\t"
+        "setp.gt.f64 pr2, %5, %13;\n\t"
         "setp.gt.f64 pc, %1, %17;\n\t"
+        "setp.gt.f64 pc2, %5, %17;\n\t"
+        "setp.gt.or.f64 pr, %2, %10, pr;\n\t"
+        "setp.gt.or.f64 pr2, %6, %14, pr2;\n\t"
         "setp.gt.or.f64 pc, %2, %17, pc;\n\t"
+        "setp.gt.or.f64 pc2, %6, %17, pc2;\n\t"
+        "setp.gt.or.f64 pr, %3, %11, pr;\n\t"
+        "setp.gt.or.f64 pr2, %7, %15, pr2;\n\t"
         "setp.gt.or.f64 pc, %3, %17, pc;\n\t"
+        "setp.gt.or.f64 pc2, %7, %17, pc2;\n\t"
+        "setp.gt.or.f64 pr, %4, %12, pr;\n\t"
+        "setp.gt.or.f64 pr2, %8, %16, pr2;\n\t"
         "setp.gt.or.f64 pc, %4, %17, pc;\n\t"
-        "setp.gt.or.f64 pc, %5, %17, pc;\n\t"
-        "setp.gt.or.f64 pc, %6, %17, pc;\n\t"
-        "setp.gt.or.f64 pc, %7, %17, pc;\n\t"
-        "setp.gt.or.f64 pc, %8, %17, pc;\n\t"
+        "setp.gt.or.f64 pc2, %8, %17, pc2;\n\t"
+        "or.pred pr, pr, pr2;\n\t"
+        "or.pred pc, pc, pc2;\n\t"
         "vote.sync.any.pred qr, pr, 0xffffffff;\n\t"
         "vote.sync.any.pred qc, pc, 0xffffffff;\n\t"
         "selp.u32 %0, 1, 0, qr;\n\t"
