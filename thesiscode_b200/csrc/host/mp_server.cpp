@@ -4,9 +4,10 @@
 // memory they need (scratch + their resident result) fits in its budget: the
 // waiting request with the fewest cells first, so that under load a small
 // request does not queue behind large ones for a slot, except that a request
-// that has waited kAgeLimitS goes before any other, so none starves.  A finished profile stays in device memory until the client
-// collects it, and its memory counts against the budget until then.  A request
-// larger than the whole budget is rejected at submission.  No counterpart in
+// that has waited kAgeLimitS goes before any other, so none starves.  A
+// finished profile stays in device memory until the client collects it, and
+// its memory counts against the budget until then.  A request larger than the
+// whole budget is rejected at submission.  No counterpart in
 // the reference (one join per process there).
 //
 // FP32 re-anchored form: one scheduler thread runs the admitted requests as
@@ -32,6 +33,7 @@
 #include <deque>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -68,7 +70,10 @@ struct mp_server {
     std::mutex mu;
     std::condition_variable cv_work;  // workers wait for admissions
     std::condition_variable cv_done;  // clients wait for completions
-    std::deque<int64_t> waiting;      // submitted, not admitted (arrival order)
+    // submitted, not admitted: by (cells, id) for shortest-first admission and
+    // by id (= arrival order) for the age limit
+    std::set<std::pair<double, int64_t>> waiting;
+    std::set<int64_t> waiting_by_age;
     std::deque<int64_t> admitted;     // admitted, not started
     std::unordered_map<int64_t, std::unique_ptr<Request>> reqs;
     size_t in_use = 0;  // bytes of admitted + resident requests
@@ -107,20 +112,24 @@ void admit_locked(mp_server* s) {
     const Clock::time_point now = Clock::now();
     while (!s->waiting.empty() && s->free_slots > 0) {
         auto fits = [&](const Request* q) { return s->in_use + q->need <= s->budget || s->in_use == 0; };
-        auto pick = s->waiting.begin();
-        Request* head = s->reqs[*pick].get();
-        if (std::chrono::duration<double>(now - head->submitted).count() >= kAgeLimitS) {
-            if (!fits(head)) break;
+        Request* r = s->reqs[*s->waiting_by_age.begin()].get();  // the oldest
+        if (std::chrono::duration<double>(now - r->submitted).count() >= kAgeLimitS) {
+            if (!fits(r)) break;
         } else {
-            pick = s->waiting.end();
-            for (auto it = s->waiting.begin(); it != s->waiting.end(); ++it) {
-                const Request* q = s->reqs[*it].get();
-                if (fits(q) && (pick == s->waiting.end() || q->cells < s->reqs[*pick]->cells)) pick = it;
+            // the fewest cells among those that fit; the first one nearly always
+            // does (a request's memory grows with its length, as its cells do)
+            r = nullptr;
+            for (const auto& e : s->waiting) {
+                Request* q = s->reqs[e.second].get();
+                if (fits(q)) {
+                    r = q;
+                    break;
+                }
             }
-            if (pick == s->waiting.end()) break;
+            if (!r) break;
         }
-        Request* r = s->reqs[*pick].get();
-        s->waiting.erase(pick);
+        s->waiting.erase({r->cells, r->id});
+        s->waiting_by_age.erase(r->id);
         s->in_use += r->need;
         r->accounted = r->need;
         --s->free_slots;
@@ -453,7 +462,8 @@ int mp_server_submit(mp_server* s, const double* A, int64_t n, int64_t m, int64_
     }
     const int64_t id = r->id;
     s->reqs[id] = std::move(r);
-    s->waiting.push_back(id);
+    s->waiting.insert({s->reqs[id]->cells, id});
+    s->waiting_by_age.insert(id);
     admit_locked(s);
     return MP_OK;
 }
@@ -535,6 +545,7 @@ int mp_server_destroy(mp_server* s) {
         std::lock_guard<std::mutex> lk(s->mu);
         s->stop = true;
         s->waiting.clear();
+        s->waiting_by_age.clear();
     }
     s->cv_work.notify_all();
     for (auto& t : s->workers) t.join();
