@@ -160,16 +160,24 @@ constexpr unsigned kFp32GroupBit = 0x80000000u;
 // i, ties to the smaller index; NaN (flat) candidates never win; -1 when none
 // qualifies.  A, mean and norm (inverse centred norms) as in the tile kernel;
 // A holds at least kPickSlots - 1 values of padding past the series.  About
-// kPickSlots * m FMAs.
+// kPickSlots * m FMAs.  Host-callable too, so the candidate rules can be
+// checked without a GPU.
 constexpr int kPickSpan = 4;
 constexpr int kPickSlots = 8 + 2 * kPickSpan;
-__device__ inline int64_t fp32_pick_neighbour(const double* A, const double* mean,
-                                              const double* norm, int64_t m, int64_t PL,
-                                              int64_t g_lo, int64_t g_hi, int64_t i, int64_t lo,
-                                              int n) {
+__host__ __device__ inline double pick_fma(double a, double b, double c) {
+#ifdef __CUDA_ARCH__
+    return __fma_rn(a, b, c);
+#else
+    return std::fma(a, b, c);
+#endif
+}
+__host__ __device__ inline int64_t fp32_pick_neighbour(const double* A, const double* mean,
+                                                       const double* norm, int64_t m, int64_t PL,
+                                                       int64_t g_lo, int64_t g_hi, int64_t i,
+                                                       int64_t lo, int n) {
     constexpr int W = kPickSlots;
-    const int64_t hi = min(lo + (int64_t)n, PL);
-    lo = max(lo, (int64_t)0);
+    const int64_t hi = lo + (int64_t)n < PL ? lo + (int64_t)n : PL;
+    lo = lo > 0 ? lo : 0;
     double c[W], w[W];
 #pragma unroll
     for (int a = 0; a < W; ++a) c[a] = 0.0;
@@ -185,14 +193,14 @@ __device__ inline int64_t fp32_pick_neighbour(const double* A, const double* mea
             const double x = A[i + t + k] - mi;
             sx += x;
 #pragma unroll
-            for (int a = 0; a < W; ++a) c[a] = __fma_rn(x, w[(k + a) % W], c[a]);
+            for (int a = 0; a < W; ++a) c[a] = pick_fma(x, w[(k + a) % W], c[a]);
         }
     }
     for (; t < m; ++t) {
         const double x = A[i + t] - mi;
         sx += x;
 #pragma unroll
-        for (int a = 0; a < W; ++a) c[a] = __fma_rn(x, A[lo + t + a], c[a]);
+        for (int a = 0; a < W; ++a) c[a] = pick_fma(x, A[lo + t + a], c[a]);
     }
     // sum_t x_t (A[q+t] - mean_q) = c - mean_q * sum_t x_t; the common factor
     // norm[i] > 0 does not change the ranking
