@@ -506,8 +506,16 @@ constexpr int fp32_smem_bytes() {
 #define MPGPU_FP32_MIN_BLOCKS 3  // 3 x 4 warps per SM (measured best of 2, 3, 4)
 #endif
 
+// CTAs per SM: group keys need fewer registers (no per-cell tags), and at 4
+// CTAs (128 registers) that instantiation ran faster than at 3 (c2 guarded
+// join 175 ms against 178); the tagged one spills more there and ran slower.
+template <bool GROUP>
+constexpr int fp32_blocks_per_sm() {
+    return GROUP ? 4 : MPGPU_FP32_MIN_BLOCKS;
+}
+
 template <int R, bool GROUP>
-__global__ void __launch_bounds__(32 * kFp32WarpsPerBlock, MPGPU_FP32_MIN_BLOCKS)
+__global__ void __launch_bounds__(32 * kFp32WarpsPerBlock, fp32_blocks_per_sm<GROUP>())
     fp32_join_kernel(const Fp32TileParams* __restrict__ series, int nseries, int64_t total,
                      unsigned long long* __restrict__ counter) {
     extern __shared__ __align__(128) char smem_fp32[];
@@ -583,7 +591,8 @@ void launch_fp32_join(const Fp32TileParams* series_dev, int nseries, int64_t tot
         configured.fetch_or(bit, std::memory_order_release);
     }
     const int64_t want = (total + kFp32WarpsPerBlock - 1) / kFp32WarpsPerBlock;
-    const int64_t blocks = std::min<int64_t>(want, (int64_t)sm_count() * MPGPU_FP32_MIN_BLOCKS);
+    const int64_t blocks = std::min<int64_t>(
+        want, (int64_t)sm_count() * (group ? fp32_blocks_per_sm<true>() : fp32_blocks_per_sm<false>()));
     if (blocks > 0 && group)
         fp32_join_kernel<R, true><<<(unsigned)blocks, 32 * kFp32WarpsPerBlock, fp32_smem_bytes<R>(), s>>>(
             series_dev, nseries, total, counter);
